@@ -1,0 +1,438 @@
+"""Benchmark: incoherent closest-hit Mrays/s on a 2,097,152-triangle heightfield.
+
+Workload (one step = one pass of the closest-hit kernel over one batch):
+  scene  heightfield 1024 x 1024 quads (2,097,152 triangles), y = 0.2 fBm
+         (6 octaves, seeded), coordinates x1000 (the scale at which the
+         reference's Cross() clamp does not act on ordinary geometry and its
+         results are pinned bit-exact), FP32.
+  rays   4,194,304 per step: 1,048,576 primary rays (1024 x 1024 top-down
+         pinhole camera) + 3,145,728 cosine-weighted diffuse secondaries,
+         three from each primary hit, shuffled into one incoherent batch.
+  also   4,194,304 any-hit shadow rays toward a 0.1 x 0.1 light at height 2.0
+         (reported as anyhit_mrays_s).
+
+value: Mrays/s with rays and hits resident in HBM; timed with CUDA events on
+the launch stream, L2 flushed (256 MiB write) between timed steps; max over
+ranks; whole-job aggregate.  e2e: the same through the host-buffer C-ABI call
+(enc_intersect_closest) from pinned host memory, copies inside the timed
+region.  --gpus N runs N independent replicas (one process per GPU, each with
+its own seeded batch, no collective on the data path).
+
+--impl reference times the reference's own CPU Kdtree::intersect
+(oracle/_ref/libencore_ref.so, compiled from the reference sources; the C
+restatement in oracle/ when that library is absent) on the host cores, on a
+bounded sample of the same ray mix.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SCALE = 1000.0
+RES = 1024
+LIGHT = np.array([0.5, 2.0, 0.5]) * SCALE
+METRIC = "Mrays/s incoherent closest-hit, 2M tris"
+WORKLOAD = "heightfield1024_x1000_4M_incoherent"
+CPU_SAMPLE = 65536  # rays per CPU step: 16384 primaries + 3 secondaries each
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# inputs
+
+def make_scene(seed: int) -> np.ndarray:
+    from encore_b200 import scenes
+    return scenes.heightfield(res=RES, seed=seed, scale=SCALE)
+
+
+def primary_rays(res: int) -> np.ndarray:
+    from encore_b200 import scenes
+    return scenes.camera_rays(res, res, eye=np.array([0.5, 1.3, 0.5]) * SCALE,
+                              look=np.array([0.5, 0.0, 0.5]) * SCALE, up=(0.0, 0.0, 1.0),
+                              fov_deg=40.0)
+
+
+def mixed_batch(tris, prim, hits, seed: int) -> np.ndarray:
+    """Primaries + 3 diffuse secondaries per primary hit, shuffled."""
+    from encore_b200 import scenes
+    sec = scenes.diffuse_rays(tris, prim, hits["tri"], hits["u"], hits["v"], per_hit=3,
+                              seed=seed, offset=1e-4 * SCALE)
+    rays = np.concatenate([prim, sec])
+    perm = np.random.default_rng(seed + 1).permutation(len(rays))
+    return np.ascontiguousarray(rays[perm])
+
+
+def shadow_batch(tris, rays, hits, n: int, seed: int) -> np.ndarray:
+    from encore_b200 import scenes
+    h = hits["tri"] >= 0
+    pts = scenes.hit_points(tris, rays[h], hits["tri"][h], hits["u"][h], hits["v"][h])
+    reps = int(np.ceil(n / max(1, len(pts))))
+    pts = np.tile(pts, (reps, 1))[:n]
+    return scenes.shadow_rays(pts, seed=seed, light_center=LIGHT, light_size=0.1 * SCALE,
+                              offset=0.01 * SCALE)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm
+
+def cpu_reference_rate(tris, rays_sample, steps: int = 1, warmup: int = 0):
+    """Times the reference's CPU Kdtree::intersect on all host threads.
+    Returns (Mrays/s over `steps` timed passes, kind, cores, build seconds)."""
+    from oracle import bindings as ob
+    lib = ob.reference()
+    nthreads = os.cpu_count() or 1
+    r6 = np.ascontiguousarray(np.concatenate([rays_sample[:, 0:3], rays_sample[:, 4:7]], axis=1))
+    n = len(r6)
+    tid = np.empty(n, np.int32)
+    t = np.empty(n, np.float32)
+    if lib is not None:
+        import ctypes as C
+        bs = C.c_double()
+        h = lib.encref_scene_create(tris.ctypes.data, len(tris), 0, C.byref(bs))
+        build_s = bs.value
+
+        def run():
+            lib.encref_closest(h, r6.ctypes.data, n, tid.ctypes.data, t.ctypes.data, None, None,
+                               nthreads)
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        kd = ob.PortKd(tris)
+        build_s = time.perf_counter() - t0
+
+        def run():
+            kd.closest(rays_sample, clamp=True, nthreads=nthreads)
+        kind = "port"
+    for _ in range(warmup):
+        run()
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    rate = n * len(times) / sum(times) / 1e6
+    return rate, kind, nthreads, build_s, times
+
+
+def cpu_sample(tris, prim_res: int = 128, seed: int = 7) -> np.ndarray:
+    """CPU_SAMPLE rays of the same mix: primaries of a prim_res^2 camera over
+    the same view, their hits from the CPU reference path, 3 secondaries each."""
+    from oracle import bindings as ob
+    from encore_b200 import scenes
+    prim = scenes.camera_rays(prim_res, prim_res, eye=np.array([0.5, 1.3, 0.5]) * SCALE,
+                              look=np.array([0.5, 0.0, 0.5]) * SCALE, up=(0.0, 0.0, 1.0),
+                              fov_deg=40.0)
+    if ob.reference() is not None:
+        hits, _ = ob.ref_closest(tris, prim, kind=0)
+    else:
+        hits = ob.PortKd(tris).closest(prim, clamp=True)
+    return mixed_batch(tris, prim, hits, seed)[:CPU_SAMPLE]
+
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    tris = make_scene(seed=1)
+    sample = cpu_sample(tris)
+    rate, kind, cores, build_s, times = cpu_reference_rate(tris, sample, steps=args.steps,
+                                                           warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(rate, 6), "unit": "Mrays/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_rays_per_step": int(len(sample)),
+                   "accelerator": "reference Kdtree (spatial median)"},
+        "cpu_baseline": {"value": round(rate, 6), "unit": "Mrays/s", "cores": cores, "kind": kind,
+                         "sample": f"{len(sample)} rays of the 1:3 primary/diffuse mix per step, "
+                                   f"Kdtree::intersect on {cores} host threads; build "
+                                   f"{build_s:.1f} s not timed"},
+        "e2e": {"value": round(rate, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+
+def read_profile_traffic() -> float | None:
+    p = ROOT / "profiles" / "wbvh_closest_heightfield_traffic.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_ray:"):
+            return float(ln.split(":", 1)[1])
+    return None
+
+
+def run_engine_arm(args, rank: int, world: int) -> None:
+    import torch
+    import torch.distributed as dist
+    from encore_b200 import Accelerator, HIT_DTYPE, LaunchConfig
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", dev),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+
+    seed = 1 + rank
+    t0 = time.perf_counter()
+    tris = make_scene(seed=1)  # every replica serves the same scene
+    prim = primary_rays(RES)
+    acc = Accelerator("wbvh", width=args.width, max_leaf_tris=args.leaf, device=dev).build(tris)
+    info = acc.info()
+    launch = LaunchConfig(block_threads=args.block, blocks_per_sm=args.bps, chunk=args.chunk,
+                          stack_depth=args.stack)
+    ph = acc.intersect(prim)
+    rays = mixed_batch(tris, prim, ph, seed=100 + seed)
+    n = len(rays)
+    hits_ref = acc.intersect(rays)
+    shadow = shadow_batch(tris, rays, hits_ref, n, seed=200 + seed)
+    log(f"[rank {rank}] inputs ready in {time.perf_counter() - t0:.1f}s: {n} rays, "
+        f"{info['ntris']} tris, {info['nnodes']} nodes, build {info['build_seconds']:.2f}s")
+
+    stream = torch.cuda.current_stream()
+    d_rays = torch.from_numpy(rays).to(dev)
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device=dev)
+    d_shadow = torch.from_numpy(shadow).to(dev)
+    d_occ = torch.empty(n, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def closest():
+        acc.intersect_device(d_rays, n, d_hits, launch=launch, stream=stream)
+
+    def anyhit():
+        acc.occluded_device(d_shadow, n, d_occ, launch=launch, stream=stream)
+
+    def timed(fn, steps):
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    for _ in range(args.warmup):
+        closest()
+        anyhit()
+    acc.check(stream)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = timed(closest, args.steps)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    acc.check(stream)
+    ms_any = timed(anyhit, args.steps)
+    acc.check(stream)
+
+    total_ms = sum(ms)
+    if world > 1:
+        tt = torch.tensor([total_ms, sum(ms_any)], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms, any_ms = tt.tolist()
+    else:
+        any_ms = sum(ms_any)
+    ms_step = total_ms / args.steps
+    value = world * n * args.steps / (total_ms * 1e-3) / 1e6
+    any_value = world * n * args.steps / (any_ms * 1e-3) / 1e6
+
+    # parity spot check of the timed output against the untimed host-form call
+    got = d_hits.cpu().numpy()
+    assert np.array_equal(got[:, 0], hits_ref["tri"]), "timed kernel output differs"
+
+    # algorithmic bytes per ray from the engine's own traversal counts
+    d_vis = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    acc.count_visits(d_rays, n, d_vis, stream=stream)
+    vis = d_vis.cpu().numpy().astype(np.int64)
+    node_b = info["node_bytes"] / max(1, info["nnodes"])
+    nodes_per_ray = vis[:, 0].mean()
+    tris_per_ray = vis[:, 1].mean()
+    bytes_per_ray = 32 + 16 + nodes_per_ray * node_b + tris_per_ray * 48
+    launch_s = ms_step * 1e-3
+    achieved = bytes_per_ray * n / launch_s / 1e9
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dram_per_ray = read_profile_traffic()
+
+    # e2e: host-buffer C-ABI call, pinned buffers, copies inside the timed region
+    h_rays = torch.from_numpy(rays).pin_memory()
+    h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory()
+    h_rays_np = h_rays.numpy()
+    h_hits_np = h_hits.numpy().view(HIT_DTYPE).reshape(n)
+    for _ in range(min(2, args.warmup)):
+        acc.intersect(h_rays_np, launch=launch, stream=stream, out=h_hits_np)
+    if world > 1:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        acc.intersect(h_rays_np, launch=launch, stream=stream, out=h_hits_np)
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = tt.item()
+    e2e_value = world * n * args.steps / (e2e_total * 1e-3) / 1e6
+    assert np.array_equal(h_hits_np["tri"], hits_ref["tri"])
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        sample = cpu_sample(tris)
+        rate, kind, cores, build_s, _ = cpu_reference_rate(tris, sample, steps=1, warmup=0)
+        cpu = {"value": round(rate, 6), "unit": "Mrays/s", "cores": cores, "kind": kind,
+               "sample": f"{len(sample)} rays of the same 1:3 primary/diffuse mix (16384 "
+                         f"primaries of a 128x128 camera + 3 secondaries each), reference "
+                         f"Kdtree::intersect on {cores} host threads; Kdtree build "
+                         f"{build_s:.1f} s not timed"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded fBm heightfield, pinhole + cosine-diffuse rays)",
+            "config": {"workload": WORKLOAD, "triangles": int(info["ntris"]),
+                       "rays_per_step": n, "scale": SCALE, "accelerator":
+                       f"wbvh{info['width']} quantised 8-bit, leaf<={args.leaf}",
+                       "l2": "flushed (256 MiB write) between timed steps",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                         "peak_source": peak_src,
+                         "traffic": (round(dram_per_ray * n) if dram_per_ray else None),
+                         "bytes_per_ray": round(bytes_per_ray, 1),
+                         "nodes_per_ray": round(float(nodes_per_ray), 2),
+                         "tris_per_ray": round(float(tris_per_ray), 2)},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(rays.nbytes), "d2h_bytes_per_step": int(n * 16)},
+            "anyhit_mrays_s": round(any_value, 3),
+            "build_seconds": round(info["build_seconds"], 3),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    acc.destroy()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--width", type=int, default=8)
+    ap.add_argument("--leaf", type=int, default=3)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--bps", type=int, default=0)
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--stack", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up below 3 steps is not a valid measurement; using 3")
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_engine_arm(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,126 @@
+"""ctypes binding of ``include/encore_b200.h``.
+
+The library is loaded from the package directory.  There is no fallback: if
+``libencore_b200.so`` is missing or fails to load, every engine call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libencore_b200.so"
+
+ENC_OK = 0
+ENC_ERR_INVALID_ARG = 1
+ENC_ERR_CUDA = 2
+ENC_ERR_OUT_OF_MEMORY = 3
+ENC_ERR_WATCHDOG = 4
+ENC_ERR_BUDGET = 5
+ENC_ERR_NOT_READY = 6
+ENC_ERR_CANCELLED = 7
+ENC_ERR_UNSUPPORTED = 8
+
+ENC_ACCEL_WBVH = 0
+ENC_ACCEL_KDTREE = 1
+ENC_PRED_REFERENCE = 0
+ENC_PRED_NOCLAMP = 1
+ENC_GATHER_IGNORE_NORMAL = 1
+
+_STATUS_NAMES = {
+    1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "watchdog",
+    5: "over budget", 6: "not ready", 7: "cancelled", 8: "unsupported",
+}
+
+
+class EncoreError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {_STATUS_NAMES.get(status, status)} ({status}): {msg}")
+        self.status = status
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("width", C.c_int32), ("max_leaf_tris", C.c_int32),
+                ("predicate", C.c_int32)]
+
+
+class LaunchOpts(C.Structure):
+    _fields_ = [("block_threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk", C.c_int32),
+                ("stack_depth", C.c_int32)]
+
+
+class AccelInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("width", C.c_int32), ("predicate", C.c_int32),
+                ("ntris", C.c_uint32), ("nnodes", C.c_uint32), ("node_bytes", C.c_uint64),
+                ("tri_bytes", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("build_seconds", C.c_double), ("scene_lo", C.c_float * 3),
+                ("scene_hi", C.c_float * 3)]
+
+
+P = C.c_void_p
+F = C.POINTER(C.c_float)
+
+# name -> (restype, argtypes); every symbol include/*.h declares.
+SIGNATURES = {
+    "enc_abi_version": (C.c_int32, []),
+    "enc_last_error": (C.c_char_p, []),
+    "enc_device_count": (C.c_int32, [C.POINTER(C.c_int32)]),
+    "enc_scene_create": (C.c_int32, [P, C.c_uint32, C.POINTER(P)]),
+    "enc_scene_destroy": (C.c_int32, [P]),
+    "enc_accel_build": (C.c_int32, [P, C.POINTER(BuildOpts), C.c_int32, C.POINTER(P)]),
+    "enc_accel_destroy": (C.c_int32, [P]),
+    "enc_accel_info_get": (C.c_int32, [P, C.POINTER(AccelInfo)]),
+    "enc_intersect_closest": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_intersect_any": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_intersect_any_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_accel_check": (C.c_int32, [P, P]),
+    "enc_accel_count_visits": (C.c_int32, [P, P, C.c_size_t, P, P]),
+    "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
+    "enc_photonmap_destroy": (C.c_int32, [P]),
+    "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),
+    "enc_photonmap_radiance_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),
+    "enc_photonmap_nearest": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P, P, P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: os.PathLike | None = None):
+    """Loads (once) and returns the engine library; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise RuntimeError(
+                f"{p} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "(the engine has no CPU fallback)")
+        lib = C.CDLL(str(p))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(status: int, where: str) -> None:
+    if status != ENC_OK:
+        msg = load().enc_last_error()
+        raise EncoreError(status, where, msg.decode() if msg else "")
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array, torch tensor or raw int pointer."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

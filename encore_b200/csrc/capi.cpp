@@ -1,0 +1,600 @@
+// C ABI of the ray-query engine: handle management, device upload, launches
+// and status checks.  Everything the reference's callers reach through
+// AccelerationStructure / PhotonMap enters here.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "photon.h"
+
+struct enc_scene_s {
+  std::vector<float> verts;
+  uint32_t ntris = 0;
+};
+
+struct enc_accel_s {
+  enc::DevAccel dev;
+  std::mutex mu;  // serialises the host-buffer forms (shared staging buffers)
+  void* d_stage_in = nullptr;
+  void* d_stage_out = nullptr;
+  size_t stage_in_bytes = 0, stage_out_bytes = 0;
+};
+
+struct enc_photonmap_s {
+  enc::DevPhotonMap dev;
+  std::mutex mu;
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+};
+
+namespace enc {
+
+namespace {
+thread_local std::string g_err;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Makes `device` current for the scope and restores the caller's device.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) ok = cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+enc_status cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? ENC_ERR_OUT_OF_MEMORY : ENC_ERR_CUDA;
+}
+
+#define ENC_CUDA(call, what)                 \
+  do {                                       \
+    cudaError_t e_ = (call);                 \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t count) {
+  *dst = nullptr;
+  if (count == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc((void**)dst, count * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+void free_dev(DevAccel& a) {
+  cudaFree(a.d_nodes);
+  cudaFree(a.d_tris);
+  cudaFree(a.d_kd);
+  cudaFree(a.d_kd_items);
+  cudaFree(a.d_status);
+  cudaFree(a.d_counter);
+  a.d_nodes = nullptr;
+  a.d_tris = nullptr;
+  a.d_kd = nullptr;
+  a.d_kd_items = nullptr;
+  a.d_status = nullptr;
+  a.d_counter = nullptr;
+}
+
+enc_status grow(void** p, size_t* cap, size_t need) {
+  if (*cap >= need) return ENC_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t n = need + need / 4;
+  cudaError_t e = cudaMalloc(p, n);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(staging)");
+  *cap = n;
+  return ENC_OK;
+}
+
+enc_status read_status(enc_accel a, cudaStream_t s) {
+  ENC_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  uint32_t st = 0;
+  ENC_CUDA(cudaMemcpy(&st, a->dev.d_status, sizeof(st), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) {
+    cudaMemset(a->dev.d_status, 0, sizeof(uint32_t));
+    set_error("kernel stopped at a loop bound (status bits " + std::to_string(st) +
+              ": 1 = step limit, 2 = stack depth, 4 = index out of range)");
+    return ENC_ERR_WATCHDOG;
+  }
+  return ENC_OK;
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+Launch resolve_launch(const enc_launch_opts* o, int kind, int width) {
+  (void)kind;
+  Launch L;
+  L.block = 128;
+  L.blocks_per_sm = width == 8 ? 4 : 4;
+  L.chunk = 64;
+  L.stack = 48;
+  if (o) {
+    if (o->block_threads > 0) L.block = o->block_threads;
+    if (o->blocks_per_sm > 0) L.blocks_per_sm = o->blocks_per_sm;
+    if (o->chunk > 0) L.chunk = o->chunk;
+    if (o->stack_depth > 0) L.stack = o->stack_depth;
+  }
+  return L;
+}
+
+}  // namespace enc
+
+using namespace enc;
+
+extern "C" {
+
+int32_t enc_abi_version(void) { return ENC_ABI_VERSION; }
+
+const char* enc_last_error(void) { return g_err.c_str(); }
+
+enc_status enc_device_count(int32_t* count) {
+  if (!count) return ENC_ERR_INVALID_ARG;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return cuda_fail(e, "cudaGetDeviceCount");
+  }
+  *count = n;
+  return ENC_OK;
+}
+
+enc_status enc_scene_create(const float* tri_verts, uint32_t ntris, enc_scene* out) {
+  if (!out || (!tri_verts && ntris)) {
+    set_error("enc_scene_create: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  enc_scene s = new (std::nothrow) enc_scene_s();
+  if (!s) return ENC_ERR_OUT_OF_MEMORY;
+  try {
+    s->verts.assign(tri_verts, tri_verts + 9 * (size_t)ntris);
+  } catch (const std::bad_alloc&) {
+    delete s;
+    return ENC_ERR_OUT_OF_MEMORY;
+  }
+  s->ntris = ntris;
+  *out = s;
+  return ENC_OK;
+}
+
+enc_status enc_scene_destroy(enc_scene scene) {
+  delete scene;
+  return ENC_OK;
+}
+
+enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t device,
+                           enc_accel* out) {
+  if (!scene || !out) {
+    set_error("enc_accel_build: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  if (scene->ntris == 0) {
+    set_error("enc_accel_build: scene has no triangles");
+    return ENC_ERR_INVALID_ARG;
+  }
+  enc_build_opts o = {ENC_ACCEL_WBVH, 8, 3, ENC_PRED_REFERENCE};
+  if (opts) o = *opts;
+  if (o.width == 0) o.width = 8;
+  if (o.max_leaf_tris == 0) o.max_leaf_tris = 3;
+  if (o.kind != ENC_ACCEL_WBVH && o.kind != ENC_ACCEL_KDTREE) {
+    set_error("enc_accel_build: unknown kind");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (o.width != 2 && o.width != 4 && o.width != 8) {
+    set_error("enc_accel_build: width must be 2, 4 or 8");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (o.max_leaf_tris < 1 || o.max_leaf_tris > 4) {
+    set_error("enc_accel_build: max_leaf_tris must be 1..4");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (o.predicate != ENC_PRED_REFERENCE && o.predicate != ENC_PRED_NOCLAMP) {
+    set_error("enc_accel_build: unknown predicate");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    set_error("enc_accel_build: no such CUDA device");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(device);
+  if (!ds.ok) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+  enc_accel a = new (std::nothrow) enc_accel_s();
+  if (!a) return ENC_ERR_OUT_OF_MEMORY;
+  DevAccel& d = a->dev;
+  d.kind = o.kind;
+  d.width = o.width;
+  d.predicate = o.predicate;
+  d.ntris = scene->ntris;
+  d.device = device;
+  double t0 = now_s();
+  cudaError_t e = cudaSuccess;
+  try {
+    if (o.kind == ENC_ACCEL_WBVH) {
+      WBVHHost h;
+      build_wbvh(scene->verts.data(), scene->ntris, o.width, o.max_leaf_tris, &h);
+      d.nnodes = h.nnodes;
+      for (int i = 0; i < 3; ++i) {
+        d.lo[i] = h.lo[i];
+        d.hi[i] = h.hi[i];
+      }
+      uint8_t* dn = nullptr;
+      e = upload(&dn, h.nodes.data(), h.nodes.size());
+      d.d_nodes = dn;
+      if (e == cudaSuccess) e = upload(&d.d_tris, h.tris.data(), h.tris.size());
+      d.node_bytes = h.nodes.size();
+      d.tri_bytes = h.tris.size() * sizeof(DevTri);
+    } else {
+      KdHost h;
+      build_kd_reference(scene->verts.data(), scene->ntris, &h);
+      std::vector<DevTri> tris(scene->ntris);
+      make_dev_tris(scene->verts.data(), scene->ntris, nullptr, tris.data());
+      d.nnodes = (uint32_t)h.nodes.size();
+      d.kd_nitems = (uint32_t)h.items.size();
+      for (int i = 0; i < 3; ++i) {
+        d.kd_root_lo[i] = h.root_lo[i];
+        d.kd_root_hi[i] = h.root_hi[i];
+        d.lo[i] = h.root_lo[i];
+        d.hi[i] = h.root_hi[i];
+      }
+      e = upload(&d.d_kd, h.nodes.data(), h.nodes.size());
+      if (e == cudaSuccess) e = upload(&d.d_kd_items, h.items.data(), h.items.size());
+      if (e == cudaSuccess) e = upload(&d.d_tris, tris.data(), tris.size());
+      d.node_bytes = h.nodes.size() * sizeof(KdNode) + h.items.size() * sizeof(uint32_t);
+      d.tri_bytes = tris.size() * sizeof(DevTri);
+    }
+  } catch (const std::bad_alloc&) {
+    free_dev(d);
+    delete a;
+    set_error("enc_accel_build: host out of memory");
+    return ENC_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& ex) {
+    free_dev(d);
+    delete a;
+    set_error(std::string("enc_accel_build: ") + ex.what());
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
+  if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, 16);
+  if (e == cudaSuccess) e = cudaMemset(d.d_counter, 0, 16);
+  if (e != cudaSuccess) {
+    free_dev(d);
+    delete a;
+    return cuda_fail(e, "enc_accel_build: upload");
+  }
+  d.device_bytes = d.node_bytes + d.tri_bytes + 32;
+  d.build_seconds = now_s() - t0;
+  *out = a;
+  return ENC_OK;
+}
+
+enc_status enc_accel_destroy(enc_accel a) {
+  if (!a) return ENC_OK;
+  DeviceScope ds(a->dev.device);
+  free_dev(a->dev);
+  cudaFree(a->d_stage_in);
+  cudaFree(a->d_stage_out);
+  delete a;
+  return ENC_OK;
+}
+
+enc_status enc_accel_info_get(enc_accel a, enc_accel_info* info) {
+  if (!a || !info) return ENC_ERR_INVALID_ARG;
+  const DevAccel& d = a->dev;
+  info->kind = d.kind;
+  info->width = d.width;
+  info->predicate = d.predicate;
+  info->ntris = d.ntris;
+  info->nnodes = d.nnodes;
+  info->node_bytes = d.node_bytes;
+  info->tri_bytes = d.tri_bytes;
+  info->device_bytes = d.device_bytes;
+  info->build_seconds = d.build_seconds;
+  for (int i = 0; i < 3; ++i) {
+    info->scene_lo[i] = d.lo[i];
+    info->scene_hi[i] = d.hi[i];
+  }
+  return ENC_OK;
+}
+
+enc_status enc_intersect_closest_device(enc_accel a, const float* d_rays, size_t nrays,
+                                        enc_hit* d_hits, const enc_launch_opts* launch,
+                                        enc_stream stream) {
+  if (!a || (nrays && (!d_rays || !d_hits))) {
+    set_error("enc_intersect_closest_device: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays > 0xffffffffull / 2) {
+    set_error("enc_intersect_closest_device: too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(a->dev.device);
+  Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
+  if (L.block % 32 != 0 || L.block > 128 || L.stack < 4 || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 4..64)");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int e = launch_closest(a->dev, d_rays, nrays, d_hits, L, stream, nullptr);
+  if (e != 0) return cuda_fail((cudaError_t)e, "closest-hit launch");
+  return ENC_OK;
+}
+
+enc_status enc_intersect_any_device(enc_accel a, const float* d_rays, size_t nrays,
+                                    uint8_t* d_occ, const enc_launch_opts* launch,
+                                    enc_stream stream) {
+  if (!a || (nrays && (!d_rays || !d_occ))) {
+    set_error("enc_intersect_any_device: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays > 0xffffffffull / 2) {
+    set_error("enc_intersect_any_device: too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(a->dev.device);
+  Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
+  if (L.block % 32 != 0 || L.block > 128 || L.stack < 4 || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 4..64)");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int e = launch_any(a->dev, d_rays, nrays, d_occ, L, stream);
+  if (e != 0) return cuda_fail((cudaError_t)e, "any-hit launch");
+  return ENC_OK;
+}
+
+enc_status enc_intersect_closest(enc_accel a, const float* rays, size_t nrays, enc_hit* hits,
+                                 const enc_launch_opts* launch, enc_stream stream) {
+  if (!a || (nrays && (!rays || !hits))) {
+    set_error("enc_intersect_closest: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays == 0) return ENC_OK;
+  std::lock_guard<std::mutex> lk(a->mu);
+  DeviceScope ds(a->dev.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  enc_status st = grow(&a->d_stage_in, &a->stage_in_bytes, nrays * 32);
+  if (st) return st;
+  st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays * sizeof(enc_hit));
+  if (st) return st;
+  ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
+  st = enc_intersect_closest_device(a, (const float*)a->d_stage_in, nrays,
+                                    (enc_hit*)a->d_stage_out, launch, stream);
+  if (st) return st;
+  ENC_CUDA(cudaMemcpyAsync(hits, a->d_stage_out, nrays * sizeof(enc_hit), cudaMemcpyDeviceToHost, s),
+           "D2H hits");
+  return read_status(a, s);
+}
+
+enc_status enc_intersect_any(enc_accel a, const float* rays, size_t nrays, uint8_t* occ,
+                             const enc_launch_opts* launch, enc_stream stream) {
+  if (!a || (nrays && (!rays || !occ))) {
+    set_error("enc_intersect_any: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays == 0) return ENC_OK;
+  std::lock_guard<std::mutex> lk(a->mu);
+  DeviceScope ds(a->dev.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  enc_status st = grow(&a->d_stage_in, &a->stage_in_bytes, nrays * 32);
+  if (st) return st;
+  st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays);
+  if (st) return st;
+  ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
+  st = enc_intersect_any_device(a, (const float*)a->d_stage_in, nrays, (uint8_t*)a->d_stage_out,
+                                launch, stream);
+  if (st) return st;
+  ENC_CUDA(cudaMemcpyAsync(occ, a->d_stage_out, nrays, cudaMemcpyDeviceToHost, s), "D2H occluded");
+  return read_status(a, s);
+}
+
+enc_status enc_accel_check(enc_accel a, enc_stream stream) {
+  if (!a) return ENC_ERR_INVALID_ARG;
+  DeviceScope ds(a->dev.device);
+  return read_status(a, static_cast<cudaStream_t>(stream));
+}
+
+enc_status enc_accel_count_visits(enc_accel a, const float* d_rays, size_t nrays,
+                                  uint32_t* d_visits, enc_stream stream) {
+  if (!a || (nrays && (!d_rays || !d_visits))) return ENC_ERR_INVALID_ARG;
+  if (a->dev.kind != ENC_ACCEL_WBVH) {
+    set_error("enc_accel_count_visits: wide BVH only");
+    return ENC_ERR_UNSUPPORTED;
+  }
+  if (nrays == 0) return ENC_OK;
+  std::lock_guard<std::mutex> lk(a->mu);
+  DeviceScope ds(a->dev.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  enc_status st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays * sizeof(enc_hit));
+  if (st) return st;
+  Launch L = resolve_launch(nullptr, a->dev.kind, a->dev.width);
+  int e = launch_closest(a->dev, d_rays, nrays, (enc_hit*)a->d_stage_out, L, stream, d_visits);
+  if (e != 0) return cuda_fail((cudaError_t)e, "count launch");
+  return read_status(a, s);
+}
+
+// ---------------------------------------------------------------------------
+// PhotonMap
+
+enc_status enc_photonmap_create(const float* pos, const float* normal, const float* power,
+                                size_t n, int32_t caustic, int32_t device, enc_photonmap* out) {
+  if (!out || (n && (!pos || !normal || !power))) {
+    set_error("enc_photonmap_create: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  if (n > 0x7fffffffull) {
+    set_error("enc_photonmap_create: too many photons");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    set_error("enc_photonmap_create: no such CUDA device");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(device);
+  enc_photonmap m = new (std::nothrow) enc_photonmap_s();
+  if (!m) return ENC_ERR_OUT_OF_MEMORY;
+  DevPhotonMap& d = m->dev;
+  d.caustic = caustic ? 1 : 0;
+  d.device = device;
+  d.n = (uint32_t)n;
+  cudaError_t e = cudaSuccess;
+  try {
+    PhotonHost h;
+    build_photon_tree(pos, normal, power, n, &h);
+    d.nnodes = (uint32_t)h.nodes.size();
+    d.depth = h.depth;
+    e = upload(&d.d_nodes, h.nodes.data(), h.nodes.size());
+    if (e == cudaSuccess) e = upload(&d.d_pos4, h.pos4.data(), h.pos4.size());
+    if (e == cudaSuccess) e = upload(&d.d_nrm4, h.nrm4.data(), h.nrm4.size());
+    if (e == cudaSuccess) e = upload(&d.d_pow4, h.pow4.data(), h.pow4.size());
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
+    if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
+  } catch (const std::exception& ex) {
+    set_error(std::string("enc_photonmap_create: ") + ex.what());
+    e = cudaErrorMemoryAllocation;
+  }
+  if (e != cudaSuccess) {
+    cudaFree(d.d_nodes);
+    cudaFree(d.d_pos4);
+    cudaFree(d.d_nrm4);
+    cudaFree(d.d_pow4);
+    cudaFree(d.d_status);
+    delete m;
+    return cuda_fail(e, "enc_photonmap_create");
+  }
+  *out = m;
+  return ENC_OK;
+}
+
+enc_status enc_photonmap_destroy(enc_photonmap m) {
+  if (!m) return ENC_OK;
+  DeviceScope ds(m->dev.device);
+  cudaFree(m->dev.d_nodes);
+  cudaFree(m->dev.d_pos4);
+  cudaFree(m->dev.d_nrm4);
+  cudaFree(m->dev.d_pow4);
+  cudaFree(m->dev.d_status);
+  cudaFree(m->d_stage);
+  delete m;
+  return ENC_OK;
+}
+
+namespace {
+enc_status gather_args(enc_photonmap m, size_t nq, int32_t k, float max_dist, const void* a,
+                       const void* b, const void* c, const char* where) {
+  if (!m || (nq && (!a || !b || !c))) {
+    set_error(std::string(where) + ": null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (k < 0 || !(max_dist >= 0.0f) || nq > 0x7fffffffull) {
+    set_error(std::string(where) + ": k must be >= 0, max_dist >= 0");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (k > 256) {
+    set_error(std::string(where) + ": k > 256 is not built");
+    return ENC_ERR_UNSUPPORTED;
+  }
+  return ENC_OK;
+}
+
+enc_status pmap_status(enc_photonmap m, cudaStream_t s) {
+  ENC_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  uint32_t st = 0;
+  ENC_CUDA(cudaMemcpy(&st, m->dev.d_status, 4, cudaMemcpyDeviceToHost), "read status");
+  if (st) {
+    cudaMemset(m->dev.d_status, 0, 4);
+    set_error("gather stopped at a loop bound");
+    return ENC_ERR_WATCHDOG;
+  }
+  return ENC_OK;
+}
+}  // namespace
+
+enc_status enc_photonmap_radiance_device(enc_photonmap m, const float* d_qpos, const float* d_qnrm,
+                                         size_t nq, int32_t k, float max_dist, int32_t flags,
+                                         float* d_rgb, enc_stream stream) {
+  enc_status st = gather_args(m, nq, k, max_dist, d_qpos, d_qnrm, d_rgb, "enc_photonmap_radiance_device");
+  if (st) return st;
+  DeviceScope ds(m->dev.device);
+  int e = launch_radiance(m->dev, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, stream);
+  if (e) return cuda_fail((cudaError_t)e, "gather launch");
+  return ENC_OK;
+}
+
+enc_status enc_photonmap_radiance(enc_photonmap m, const float* qpos, const float* qnrm, size_t nq,
+                                  int32_t k, float max_dist, int32_t flags, float* rgb,
+                                  enc_stream stream) {
+  enc_status st = gather_args(m, nq, k, max_dist, qpos, qnrm, rgb, "enc_photonmap_radiance");
+  if (st || nq == 0) return st;
+  std::lock_guard<std::mutex> lk(m->mu);
+  DeviceScope ds(m->dev.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t b3 = nq * 3 * sizeof(float);
+  st = grow(&m->d_stage, &m->stage_bytes, 3 * b3);
+  if (st) return st;
+  float* dq = (float*)m->d_stage;
+  float* dn = dq + 3 * nq;
+  float* dr = dn + 3 * nq;
+  ENC_CUDA(cudaMemcpyAsync(dq, qpos, b3, cudaMemcpyHostToDevice, s), "H2D queries");
+  ENC_CUDA(cudaMemcpyAsync(dn, qnrm, b3, cudaMemcpyHostToDevice, s), "H2D normals");
+  int e = launch_radiance(m->dev, dq, dn, nq, k, max_dist, flags, dr, stream);
+  if (e) return cuda_fail((cudaError_t)e, "gather launch");
+  ENC_CUDA(cudaMemcpyAsync(rgb, dr, b3, cudaMemcpyDeviceToHost, s), "D2H radiance");
+  return pmap_status(m, s);
+}
+
+enc_status enc_photonmap_nearest(enc_photonmap m, const float* qpos, const float* qnrm, size_t nq,
+                                 int32_t k, float max_dist, int32_t flags, int32_t* idx, float* d2,
+                                 int32_t* count, enc_stream stream) {
+  enc_status st = gather_args(m, nq, k, max_dist, qpos, qnrm, idx, "enc_photonmap_nearest");
+  if (st || nq == 0) return st;
+  if (!d2 || !count) return ENC_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(m->mu);
+  DeviceScope ds(m->dev.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t b3 = nq * 3 * sizeof(float);
+  const size_t bk = nq * (size_t)k * 4;
+  st = grow(&m->d_stage, &m->stage_bytes, 2 * b3 + 2 * bk + nq * 4);
+  if (st) return st;
+  char* base = (char*)m->d_stage;
+  float* dq = (float*)base;
+  float* dn = (float*)(base + b3);
+  int32_t* di = (int32_t*)(base + 2 * b3);
+  float* dd = (float*)(base + 2 * b3 + bk);
+  int32_t* dc = (int32_t*)(base + 2 * b3 + 2 * bk);
+  ENC_CUDA(cudaMemcpyAsync(dq, qpos, b3, cudaMemcpyHostToDevice, s), "H2D queries");
+  ENC_CUDA(cudaMemcpyAsync(dn, qnrm, b3, cudaMemcpyHostToDevice, s), "H2D normals");
+  int e = launch_nearest(m->dev, dq, dn, nq, k, max_dist, flags, di, dd, dc, stream);
+  if (e) return cuda_fail((cudaError_t)e, "gather launch");
+  if (bk) {
+    ENC_CUDA(cudaMemcpyAsync(idx, di, bk, cudaMemcpyDeviceToHost, s), "D2H idx");
+    ENC_CUDA(cudaMemcpyAsync(d2, dd, bk, cudaMemcpyDeviceToHost, s), "D2H d2");
+  }
+  ENC_CUDA(cudaMemcpyAsync(count, dc, nq * 4, cudaMemcpyDeviceToHost, s), "D2H count");
+  return pmap_status(m, s);
+}
+
+}  // extern "C"

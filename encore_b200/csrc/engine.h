@@ -1,0 +1,134 @@
+// Internal declarations shared by the host builders, the CUDA kernels and the
+// C ABI.  Device layouts are defined here once so the builder that writes a
+// structure and the kernel that walks it agree by construction.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/encore_b200.h"
+
+namespace enc {
+
+// ---------------------------------------------------------------------------
+// Triangles on the device: 3 x float4 = 48 bytes, read with three 16-byte
+// vector loads.  e1 = v1 - v0 and e2 = v2 - v0 are precomputed on the host in
+// FP32, which yields the same floats the reference forms per test as
+// Vector3(v0, v1) and Vector3(v0, v2) (TrianglePrim.cpp:210-211).
+//   a = (v0.x, v0.y, v0.z, e1.x)
+//   b = (e1.y, e1.z, e2.x, e2.y)
+//   c = (e2.z, id as int bits, 0, 0)
+struct alignas(16) DevTri {
+  float a[4], b[4], c[4];
+};
+static_assert(sizeof(DevTri) == 48, "DevTri is three float4");
+
+// ---------------------------------------------------------------------------
+// Wide BVH node, width W in {2, 4, 8}.  Child boxes are stored as 8-bit
+// offsets from the node origin p in units of 2^(e-127) per axis, rounded
+// outward (lo floored, hi ceiled) so a decoded box always contains the
+// child's true box.
+//
+// meta[c]: 0 = empty slot; 1..8 = internal child, node index child_base +
+// (meta-1); >= 32 = leaf, triangle count meta>>5 (1..7) starting at
+// tri_base + (meta & 31).
+template <int W>
+struct WNodeLayout {
+  static constexpr int kRaw = 24 + 7 * W;
+  static constexpr int kBytes = (kRaw + 15) / 16 * 16;  // 48, 64, 80
+  static constexpr int kMetaOff = 24;
+  static constexpr int kQOff = 24 + W;  // qlo x,y,z then qhi x,y,z; W bytes each
+};
+
+struct WNodeHeader {  // first 24 bytes of every wide node
+  float p[3];
+  uint8_t e[3];
+  uint8_t nchild;
+  uint32_t child_base;
+  uint32_t tri_base;
+};
+static_assert(sizeof(WNodeHeader) == 24, "wide node header is 24 bytes");
+
+// ---------------------------------------------------------------------------
+// kd-tree node, 8 bytes.  The reference stores flags/split/count in one union
+// and the child index / primitive list pointer in another (Kdtree.h:25-58);
+// its initNode writes the axis into the two low bits of the split float
+// (Kdtree.h:47-52), so the split value its traversal reads differs from the
+// build's split position in those bits.  This layout keeps exactly that word:
+//   word0 low 2 bits == 3  -> leaf, count = word0 >> 2, word1 = first index
+//                             into the leaf-index array
+//   otherwise              -> internal, axis = word0 & 3, split = as_float(word0),
+//                             children at word1 and word1 + 1
+struct KdNode {
+  uint32_t word0;
+  uint32_t word1;
+};
+
+// ---------------------------------------------------------------------------
+// Device-resident accelerator.
+struct DevAccel {
+  int kind = 0;
+  int width = 8;
+  int predicate = 0;
+  uint32_t ntris = 0;
+  uint32_t nnodes = 0;
+  // WBVH
+  void* d_nodes = nullptr;      // nnodes * WNodeLayout<W>::kBytes
+  DevTri* d_tris = nullptr;     // WBVH: leaf order; kd: triangle-ID order
+  // kd-tree
+  KdNode* d_kd = nullptr;
+  uint32_t* d_kd_items = nullptr;  // leaf triangle IDs
+  uint32_t kd_nitems = 0;
+  float kd_root_lo[3] = {0, 0, 0}, kd_root_hi[3] = {0, 0, 0};
+  // status word written by kernels (watchdog / bounds)
+  uint32_t* d_status = nullptr;
+  uint32_t* d_counter = nullptr;  // work-queue heads (4 words)
+  size_t node_bytes = 0, tri_bytes = 0, device_bytes = 0;
+  int device = 0;
+  double build_seconds = 0;
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
+// Host results of the builders (before upload).
+struct WBVHHost {
+  int width = 8;
+  std::vector<uint8_t> nodes;  // nnodes * kBytes
+  uint32_t nnodes = 0;
+  std::vector<DevTri> tris;    // leaf order
+  float lo[3], hi[3];
+};
+
+struct KdHost {
+  std::vector<KdNode> nodes;
+  std::vector<uint32_t> items;
+  float root_lo[3], root_hi[3];  // reference root box (pos, pos + size)
+  int max_depth = 0;
+};
+
+// Builders (host).  tri_verts: 9 floats per triangle.
+void build_wbvh(const float* tri_verts, uint32_t ntris, int width, int max_leaf, WBVHHost* out);
+void build_kd_reference(const float* tri_verts, uint32_t ntris, KdHost* out);
+void make_dev_tris(const float* tri_verts, uint32_t ntris, const uint32_t* order, DevTri* out);
+
+// Launch parameters after defaults are applied.
+struct Launch {
+  int block = 128;
+  int blocks_per_sm = 4;
+  int chunk = 32;
+  int stack = 32;
+};
+Launch resolve_launch(const enc_launch_opts* o, int kind, int width);
+
+// Kernel launchers (trace.cu).  All asynchronous on `stream`.
+int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_hits,
+                   const Launch& L, void* stream, uint32_t* d_visits);
+int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
+               const Launch& L, void* stream);
+int device_sm_count(int device);
+
+// Error reporting (capi.cpp).
+void set_error(const std::string& msg);
+
+}  // namespace enc

@@ -1,0 +1,319 @@
+// Photon k-nearest gather and radiance estimate for sm_100a.
+//
+// One warp per query point.  The warp walks the photon kd-tree (photon.h)
+// front to back with a per-warp stack in shared memory; at a leaf each lane
+// tests one photon (32-photon leaves = one coalesced 16-byte load per lane per
+// array).  The k best candidates are kept in a warp-distributed bounded
+// max-heap: S = ceil(k/32) register slots per lane, slot i on lane i % 32; the
+// maximum and its owner are found with a 5-step shuffle reduction, and an
+// accepted candidate replaces it.  The search radius is max_dist^2 until k
+// photons are held and the heap maximum afterwards, as in
+// PhotonMap::GetNearestNPhotons (PhotonMap.cpp:224-297), so the result is the
+// exact k-nearest set.
+//
+// Acceptance is the reference's: FP32 dist^2 = (x*x + y*y) + z*z with separate
+// roundings, dist^2 < r^2, and the stored surface normal equal to the query
+// normal component by component unless ENC_GATHER_IGNORE_NORMAL
+// (PhotonMap.cpp:239-244).  The estimate follows GetRadianceEstimate
+// (PhotonMap.cpp:121-164): r = largest dist^2 found; weight 1 (global map) or
+// (r - d)/d (caustic map); density 1 or k / (pi r^2) with pi = 3.14159f
+// (Common.h:36); FP32 accumulation.
+#include <cuda_runtime.h>
+
+#include "../../include/encore_b200.h"
+#include "photon.h"
+
+namespace enc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarpsPerBlock = 8;
+constexpr int kStack = 32;
+constexpr unsigned kMaxSteps = 1u << 24;
+
+struct GatherParams {
+  const PNode* nodes;
+  const float4* pos4;
+  const float4* nrm4;
+  const float4* pow4;
+  const float* qpos;
+  const float* qnrm;
+  float* rgb;
+  int32_t* idx;
+  float* d2;
+  int32_t* count;
+  uint32_t* status;
+  unsigned nq;
+  int k;
+  float r2max;
+  int ignore_normal;
+  int caustic;
+};
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+
+// Max over the slots marked valid (slot index s*32 + lane < limit) and its
+// slot index; -INF / -1 if none.
+template <int S>
+__device__ __forceinline__ void warp_max(const float (&dd)[S], int lane, int limit, float& v,
+                                         int& loc) {
+  v = -INFINITY;
+  loc = -1;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int slot = s * 32 + lane;
+    if (slot < limit && (dd[s] > v || (dd[s] == v && slot > loc))) {
+      v = dd[s];
+      loc = slot;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ov = __shfl_xor_sync(kFull, v, off);
+    const int ol = __shfl_xor_sync(kFull, loc, off);
+    if (ov > v || (ov == v && ol > loc)) {
+      v = ov;
+      loc = ol;
+    }
+  }
+}
+
+template <int S, bool NEAREST>
+__global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
+  __shared__ int s_node[kWarpsPerBlock][kStack];
+  __shared__ float s_pd[kWarpsPerBlock][kStack];
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const unsigned total = gridDim.x * kWarpsPerBlock;
+  const int k = P.k;
+  for (unsigned q = blockIdx.x * kWarpsPerBlock + wib; q < P.nq; q += total) {
+    const float qx = __ldg(P.qpos + 3 * (size_t)q), qy = __ldg(P.qpos + 3 * (size_t)q + 1),
+                qz = __ldg(P.qpos + 3 * (size_t)q + 2);
+    const float nx = __ldg(P.qnrm + 3 * (size_t)q), ny = __ldg(P.qnrm + 3 * (size_t)q + 1),
+                nz = __ldg(P.qnrm + 3 * (size_t)q + 2);
+    float dd[S];
+    int ds[S];
+    int dorig[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      dd[s] = INFINITY;
+      ds[s] = 0;
+      dorig[s] = -1;
+    }
+    int count = 0;
+    float worst = INFINITY;
+    int worst_loc = -1;
+    float r2 = P.r2max;
+    int sp = 0;
+    int node = 0;
+    unsigned steps = 0;
+    while (k > 0) {
+      if (++steps > kMaxSteps) {
+        if (lane == 0) atomicOr(P.status, 1u);
+        break;
+      }
+      const int4 raw = __ldg(reinterpret_cast<const int4*>(P.nodes) + node);
+      PNode nd;
+      nd.split = __int_as_float(raw.x);
+      nd.axis = raw.y;
+      nd.begin = (unsigned)raw.z;
+      nd.end = (unsigned)raw.w;
+      if (nd.axis >= 0) {
+        const float qa = nd.axis == 0 ? qx : (nd.axis == 1 ? qy : qz);
+        const float dq = fs(qa, nd.split);
+        const int left = 2 * node + 1;
+        const int nearc = dq <= 0.0f ? left : left + 1;
+        const int farc = dq <= 0.0f ? left + 1 : left;
+        const float pd = fm(dq, dq);
+        if (pd < r2) {
+          if (sp >= kStack) {
+            if (lane == 0) atomicOr(P.status, 2u);
+            break;
+          }
+          s_node[wib][sp] = farc;
+          s_pd[wib][sp] = pd;
+          ++sp;
+          __syncwarp();
+        }
+        node = nearc;
+        continue;
+      }
+      // leaf: lane j tests photon begin + j
+      const unsigned pidx = nd.begin + (unsigned)lane;
+      bool acc = false;
+      float d2 = 0.f;
+      int orig = -1;
+      if (pidx < nd.end) {
+        const float4 p = __ldg(P.pos4 + pidx);
+        const float x = fs(qx, p.x), y = fs(qy, p.y), z = fs(qz, p.z);
+        d2 = fa(fa(fm(x, x), fm(y, y)), fm(z, z));
+        orig = __float_as_int(p.w);
+        acc = d2 < r2;
+        if (acc && !P.ignore_normal) {
+          const float4 pn = __ldg(P.nrm4 + pidx);
+          acc = (pn.x == nx) && (pn.y == ny) && (pn.z == nz);
+        }
+      }
+      unsigned m = __ballot_sync(kFull, acc);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        const float cd = __shfl_sync(kFull, d2, j);
+        const int co = __shfl_sync(kFull, orig, j);
+        const int cs = (int)nd.begin + j;
+        if (count < k) {
+          const int slot = count;
+#pragma unroll
+          for (int s = 0; s < S; ++s)
+            if (lane == (slot & 31) && s == (slot >> 5)) {
+              dd[s] = cd;
+              ds[s] = cs;
+              dorig[s] = co;
+            }
+          ++count;
+          if (count == k) {
+            warp_max<S>(dd, lane, k, worst, worst_loc);
+            r2 = worst;
+          }
+        } else if (cd < worst) {
+#pragma unroll
+          for (int s = 0; s < S; ++s)
+            if (lane == (worst_loc & 31) && s == (worst_loc >> 5)) {
+              dd[s] = cd;
+              ds[s] = cs;
+              dorig[s] = co;
+            }
+          warp_max<S>(dd, lane, k, worst, worst_loc);
+          r2 = worst;
+        }
+      }
+      // pop the next subtree that can still hold a closer photon
+      node = -1;
+      while (sp > 0) {
+        --sp;
+        if (s_pd[wib][sp] < r2) {
+          node = s_node[wib][sp];
+          break;
+        }
+      }
+      __syncwarp();
+      if (node < 0) break;
+    }
+
+    if (NEAREST) {
+      // rank = number of held entries ordered before this one (dist^2, index)
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int slot = s * 32 + lane;
+        int rank = 0;
+#pragma unroll
+        for (int s2 = 0; s2 < S; ++s2)
+          for (int l = 0; l < 32; ++l) {
+            const float od = __shfl_sync(kFull, dd[s2], l);
+            const int oo = __shfl_sync(kFull, dorig[s2], l);
+            const int oslot = s2 * 32 + l;
+            if (oslot < count && (od < dd[s] || (od == dd[s] && oo < dorig[s]))) ++rank;
+          }
+        if (slot < count) {
+          P.idx[(size_t)q * k + rank] = dorig[s];
+          P.d2[(size_t)q * k + rank] = dd[s];
+        }
+      }
+      for (int p = count + lane; p < k; p += 32) {
+        P.idx[(size_t)q * k + p] = -1;
+        P.d2[(size_t)q * k + p] = 0.f;
+      }
+      if (lane == 0) P.count[q] = count;
+    } else {
+      float R = 0.f, G = 0.f, B = 0.f;
+      if (count > 0) {
+        float r;
+        int loc;
+        warp_max<S>(dd, lane, count, r, loc);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          if (s * 32 + lane < count) {
+            const float w = P.caustic ? __fdiv_rn(fs(r, dd[s]), dd[s]) : 1.0f;
+            const float4 pw = __ldg(P.pow4 + ds[s]);
+            R = fa(R, fm(pw.x, w));
+            G = fa(G, fm(pw.y, w));
+            B = fa(B, fm(pw.z, w));
+          }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          R += __shfl_xor_sync(kFull, R, off);
+          G += __shfl_xor_sync(kFull, G, off);
+          B += __shfl_xor_sync(kFull, B, off);
+        }
+        if (P.caustic) {
+          const float dens = __fdiv_rn((float)k, fm(fm(3.14159f, r), r));
+          R = fm(R, dens);
+          G = fm(G, dens);
+          B = fm(B, dens);
+        }
+      }
+      if (lane == 0) {
+        P.rgb[3 * (size_t)q] = R;
+        P.rgb[3 * (size_t)q + 1] = G;
+        P.rgb[3 * (size_t)q + 2] = B;
+      }
+    }
+  }
+}
+
+template <bool NEAREST>
+int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, size_t nq, int k,
+                  float max_dist, int flags, float* rgb, int32_t* idx, float* d2, int32_t* count,
+                  cudaStream_t s) {
+  if (nq == 0) return 0;
+  GatherParams p;
+  p.nodes = m.d_nodes;
+  p.pos4 = reinterpret_cast<const float4*>(m.d_pos4);
+  p.nrm4 = reinterpret_cast<const float4*>(m.d_nrm4);
+  p.pow4 = reinterpret_cast<const float4*>(m.d_pow4);
+  p.qpos = qpos;
+  p.qnrm = qnrm;
+  p.rgb = rgb;
+  p.idx = idx;
+  p.d2 = d2;
+  p.count = count;
+  p.status = m.d_status;
+  p.nq = (unsigned)nq;
+  p.k = m.n == 0 ? 0 : k;
+  p.r2max = max_dist * max_dist;  // maxDistance*maxDistance in FP32 (PhotonMap.cpp:89)
+  p.ignore_normal = (flags & ENC_GATHER_IGNORE_NORMAL) ? 1 : 0;
+  p.caustic = m.caustic;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+  unsigned need = (unsigned)((nq + kWarpsPerBlock - 1) / kWarpsPerBlock);
+  unsigned grid = (unsigned)sms * 8;
+  if (grid > need) grid = need;
+  const int S = k <= 32 ? 1 : (k <= 64 ? 2 : (k <= 128 ? 4 : 8));
+  switch (S) {
+    case 1: gather_kernel<1, NEAREST><<<grid, 256, 0, s>>>(p); break;
+    case 2: gather_kernel<2, NEAREST><<<grid, 256, 0, s>>>(p); break;
+    case 4: gather_kernel<4, NEAREST><<<grid, 256, 0, s>>>(p); break;
+    default: gather_kernel<8, NEAREST><<<grid, 256, 0, s>>>(p); break;
+  }
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+int launch_radiance(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
+                    int k, float max_dist, int flags, float* d_rgb, void* stream) {
+  return launch_gather<false>(m, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, nullptr, nullptr,
+                              nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int launch_nearest(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
+                   int k, float max_dist, int flags, int32_t* d_idx, float* d_d2,
+                   int32_t* d_count, void* stream) {
+  return launch_gather<true>(m, d_qpos, d_qnrm, nq, k, max_dist, flags, nullptr, d_idx, d_d2,
+                             d_count, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace enc

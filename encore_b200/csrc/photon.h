@@ -1,0 +1,57 @@
+// Photon map: device layout shared by the host builder (photon.cpp) and the
+// gather kernel (gather.cu).
+//
+// The tree is a complete binary kd-tree over photon index ranges: every
+// internal node splits its range at the median index on the axis of the
+// range's largest extent (the reference balances at the median too,
+// PhotonMap.cpp:176-221), and leaves hold at most 32 photons, one per lane of
+// the warp that gathers a query.  Photons are stored in leaf order as SoA
+// float4 arrays so a leaf is one coalesced 512-byte read per array.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace enc {
+
+constexpr int kPhotonLeaf = 32;
+
+struct PNode {
+  float split;     // internal: split coordinate
+  int32_t axis;    // internal: 0..2; leaf: -1
+  uint32_t begin;  // photon range [begin, end)
+  uint32_t end;
+};
+
+struct PhotonHost {
+  std::vector<PNode> nodes;   // heap order: children of i at 2i+1, 2i+2
+  std::vector<float> pos4;    // x, y, z, original index (int bits)
+  std::vector<float> nrm4;    // nx, ny, nz, 0
+  std::vector<float> pow4;    // r, g, b, 0
+  int depth = 0;
+};
+
+void build_photon_tree(const float* pos, const float* nrm, const float* power, size_t n,
+                       PhotonHost* out);
+
+struct DevPhotonMap {
+  PNode* d_nodes = nullptr;
+  float* d_pos4 = nullptr;
+  float* d_nrm4 = nullptr;
+  float* d_pow4 = nullptr;
+  uint32_t* d_status = nullptr;
+  uint32_t nnodes = 0;
+  uint32_t n = 0;
+  int depth = 0;
+  int caustic = 0;
+  int device = 0;
+};
+
+// Launchers (gather.cu).  k <= 256.  Asynchronous on `stream`.
+int launch_radiance(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
+                    int k, float max_dist, int flags, float* d_rgb, void* stream);
+int launch_nearest(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
+                   int k, float max_dist, int flags, int32_t* d_idx, float* d_d2,
+                   int32_t* d_count, void* stream);
+
+}  // namespace enc

@@ -1,0 +1,199 @@
+/*
+ * encore_b200 — C ABI of the B200 ray-query engine.
+ *
+ * The engine replaces the reference's CPU query path:
+ *   - AccelerationStructure::build / intersect
+ *       (ENCORE/src/accelerators/AccelerationStructure.h:47, :63)
+ *     as implemented by Kdtree (ENCORE/src/accelerators/Kdtree.cpp:84-200, 682-784)
+ *     and Bvh (ENCORE/src/accelerators/BVH.cpp:123-187, 778-884);
+ *   - the shadow test PhotonMapperCPU::IsInShadow
+ *       (ENCORE/src/renderers/PhotonMapperCPU.cpp:1192-1207);
+ *   - PhotonMap::AddPhoton / BalanceAndConstruct / GetNearestNPhotons /
+ *     GetRadianceEstimate (ENCORE/src/renderers/PhotonMap.cpp:46-53, 167-221,
+ *     76-94 + 224-297, 121-164).
+ *
+ * Every entry point returns an enc_status; nothing throws across the ABI.
+ * Handles are thread-safe for concurrent queries on distinct streams; build
+ * and destroy calls must not race with queries on the same handle.
+ *
+ * Data formats (all FP32, little endian):
+ *   triangle soup : 9 floats per triangle (v0, v1, v2); the index in this
+ *                   array is the triangle ID (primitive-list order,
+ *                   ENCORE/src/scene/Model.cpp:255-264).
+ *   ray           : 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax), 32 bytes.
+ *                   A hit must satisfy tmin < t < tmax; the reference's own
+ *                   rays are tmin = 0, tmax = +inf (TrianglePrim.cpp:223-224).
+ *   hit           : enc_hit, 16 bytes; tri = -1 for a miss.
+ *   photon        : position (3 floats), surface normal (3), RGB power (3).
+ */
+#ifndef ENCORE_B200_H
+#define ENCORE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ENC_ABI_VERSION 1
+
+typedef int32_t enc_status;
+enum {
+  ENC_OK = 0,
+  ENC_ERR_INVALID_ARG = 1,   /* null handle/pointer, bad size, bad option */
+  ENC_ERR_CUDA = 2,          /* a CUDA runtime call failed (see enc_last_error) */
+  ENC_ERR_OUT_OF_MEMORY = 3, /* device or host allocation failed */
+  ENC_ERR_WATCHDOG = 4,      /* a kernel hit its bounded-loop limit and stopped */
+  ENC_ERR_BUDGET = 5,        /* serving: request larger than the memory budget */
+  ENC_ERR_NOT_READY = 6,     /* serving: result not complete yet */
+  ENC_ERR_CANCELLED = 7,     /* serving: request cancelled or timed out */
+  ENC_ERR_UNSUPPORTED = 8    /* option combination not built */
+};
+
+typedef struct enc_hit {
+  int32_t tri; /* triangle ID, -1 = miss */
+  float t;     /* hit distance as the FP32 predicate computes it */
+  float u;     /* alpha (barycentric of v1), TrianglePrim.cpp:219 */
+  float v;     /* beta  (barycentric of v2), TrianglePrim.cpp:220 */
+} enc_hit;
+
+typedef struct enc_scene_s* enc_scene;
+typedef struct enc_accel_s* enc_accel;
+typedef struct enc_photonmap_s* enc_photonmap;
+typedef void* enc_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+/* Accelerator kinds. */
+enum {
+  /* Flattened wide BVH, binned-SAH build, child boxes quantised to 8 bits and
+   * rounded outward.  The throughput path. */
+  ENC_ACCEL_WBVH = 0,
+  /* Flattened kd-tree built by the reference's own rules (spatial median,
+   * axis depth%3, box-overlap distribution, Kdtree.cpp:299-680) and walked in
+   * the reference's traversal order (Kdtree.cpp:682-784).  Bit-exact with the
+   * reference's Kdtree at any scene scale, including its degenerate cases. */
+  ENC_ACCEL_KDTREE = 1
+};
+
+/* Predicate modes. */
+enum {
+  /* The reference's triangle test op for op: FP32, no FMA contraction, IEEE
+   * division, Cross() components with |c| < 0.001 clamped to 0
+   * (ENCORE/src/math/Vector3.h:148-161, Vector3.cpp:126-140). */
+  ENC_PRED_REFERENCE = 0,
+  /* The same FP32 operation order without the clamp (geometric mode). */
+  ENC_PRED_NOCLAMP = 1
+};
+
+typedef struct enc_build_opts {
+  int32_t kind;          /* ENC_ACCEL_* */
+  int32_t width;         /* WBVH branching factor: 2, 4 or 8 (0 = 8) */
+  int32_t max_leaf_tris; /* WBVH triangles per leaf, 1..4 (0 = 3) */
+  int32_t predicate;     /* ENC_PRED_* */
+} enc_build_opts;
+
+typedef struct enc_launch_opts {
+  int32_t block_threads; /* threads per block, multiple of 32 (0 = tuned default) */
+  int32_t blocks_per_sm; /* persistent CTAs per SM (0 = tuned default) */
+  int32_t chunk;         /* rays a warp takes from the queue per refill (0 = 32) */
+  int32_t stack_depth;   /* traversal stack entries per ray (0 = 32; max 64) */
+} enc_launch_opts;
+
+typedef struct enc_accel_info {
+  int32_t kind, width, predicate;
+  uint32_t ntris;
+  uint32_t nnodes;
+  uint64_t node_bytes;
+  uint64_t tri_bytes;
+  uint64_t device_bytes; /* total device memory held by the accelerator */
+  double build_seconds;  /* host build + upload wall time */
+  float scene_lo[3], scene_hi[3];
+} enc_accel_info;
+
+/* Library / device. */
+int32_t enc_abi_version(void);
+const char* enc_last_error(void); /* thread-local message of the last failure */
+enc_status enc_device_count(int32_t* count);
+
+/* Scene: a triangle soup copied to host memory owned by the handle.
+ * Replaces the IModel primitive lists that build() walks (Kdtree.cpp:99-114). */
+enc_status enc_scene_create(const float* tri_verts, uint32_t ntris, enc_scene* out);
+enc_status enc_scene_destroy(enc_scene scene);
+
+/* AccelerationStructure::build (AccelerationStructure.h:47).  Builds on the
+ * host, uploads to `device`, returns an accelerator resident in HBM.  The
+ * scene may be destroyed afterwards. */
+enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t device,
+                           enc_accel* out);
+enc_status enc_accel_destroy(enc_accel accel);
+enc_status enc_accel_info_get(enc_accel accel, enc_accel_info* info);
+
+/* AccelerationStructure::intersect (AccelerationStructure.h:63), batched.
+ * Host-buffer form: copies rays in, traces, copies hits out, synchronises
+ * `stream` before returning. */
+enc_status enc_intersect_closest(enc_accel accel, const float* rays, size_t nrays, enc_hit* hits,
+                                 const enc_launch_opts* launch, enc_stream stream);
+/* Device-buffer form: rays and hits already in device memory; asynchronous
+ * on `stream`.  Kernel status is checked by enc_stream_check. */
+enc_status enc_intersect_closest_device(enc_accel accel, const float* d_rays, size_t nrays,
+                                        enc_hit* d_hits, const enc_launch_opts* launch,
+                                        enc_stream stream);
+
+/* Shadow / any-hit: occluded[i] = 1 iff some triangle is hit with
+ * tmin < t < tmax.  This is the boolean PhotonMapperCPU::IsInShadow
+ * computes as closest-hit && hitTime < distToLight (PhotonMapperCPU.cpp:1204),
+ * answered with an early exit. */
+enc_status enc_intersect_any(enc_accel accel, const float* rays, size_t nrays, uint8_t* occluded,
+                             const enc_launch_opts* launch, enc_stream stream);
+enc_status enc_intersect_any_device(enc_accel accel, const float* d_rays, size_t nrays,
+                                    uint8_t* d_occluded, const enc_launch_opts* launch,
+                                    enc_stream stream);
+
+/* Waits for `stream` and reports ENC_ERR_WATCHDOG if any kernel this library
+ * launched on this accelerator stopped at its loop bound since the last check. */
+enc_status enc_accel_check(enc_accel accel, enc_stream stream);
+
+/* Per-ray traversal counters of the last enc_accel_count_visits call:
+ * visits[2*i] = nodes visited, visits[2*i+1] = triangles tested. Used for the
+ * bytes-per-ray roofline (device buffers, closest-hit traversal). */
+enc_status enc_accel_count_visits(enc_accel accel, const float* d_rays, size_t nrays,
+                                  uint32_t* d_visits, enc_stream stream);
+
+/* PhotonMap: AddPhoton x n followed by BalanceAndConstruct
+ * (PhotonMap.cpp:46-53, 167-221).  caustic != 0 selects the caustic-map
+ * estimate (cone weight and N/(pi r^2), PhotonMap.cpp:147, 157). */
+enc_status enc_photonmap_create(const float* pos, const float* normal, const float* power,
+                                size_t nphotons, int32_t caustic, int32_t device,
+                                enc_photonmap* out);
+enc_status enc_photonmap_destroy(enc_photonmap map);
+
+/* Gather flags. */
+enum {
+  /* Accept photons regardless of normal (IGNORE_NORMAL = true, PhotonMap.cpp:23).
+   * Default: a photon counts only if its stored surface normal equals the
+   * query normal exactly (PhotonMap.cpp:244). */
+  ENC_GATHER_IGNORE_NORMAL = 1
+};
+
+/* GetRadianceEstimate (PhotonMap.cpp:121-164) for nq query points
+ * (position + normal, 3 floats each); rgb gets 3 floats per query. */
+enc_status enc_photonmap_radiance(enc_photonmap map, const float* qpos, const float* qnrm,
+                                  size_t nq, int32_t k, float max_dist, int32_t flags,
+                                  float* rgb, enc_stream stream);
+enc_status enc_photonmap_radiance_device(enc_photonmap map, const float* d_qpos,
+                                         const float* d_qnrm, size_t nq, int32_t k,
+                                         float max_dist, int32_t flags, float* d_rgb,
+                                         enc_stream stream);
+/* GetNearestNPhotons (PhotonMap.cpp:76-94): for each query the indices (into
+ * the arrays given to enc_photonmap_create) and squared distances of the k
+ * nearest accepted photons, ascending by distance, padded with -1; count[i]
+ * is how many were found. */
+enc_status enc_photonmap_nearest(enc_photonmap map, const float* qpos, const float* qnrm,
+                                 size_t nq, int32_t k, float max_dist, int32_t flags,
+                                 int32_t* idx, float* d2, int32_t* count, enc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ENCORE_B200_H */

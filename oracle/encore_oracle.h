@@ -1,0 +1,75 @@
+/*
+ * Test oracle: a CPU restatement, in plain C, of the reference's ray-query
+ * path.  It is the checker for the engine's CUDA kernels and is used only by
+ * tests/, __graft_entry__.smoke() and the CPU arm of bench.py.  The engine
+ * never links or calls it.
+ *
+ * Parity pins: tests/test_oracle_pins.py checks every function here against
+ * the reference itself (oracle/_ref/libencore_ref.so, compiled from the
+ * reference's own sources) and against the committed golden vectors in
+ * tests/golden/, which that library produced.
+ *
+ * Rays are 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax); a hit needs
+ * tmin < t < tmax (the reference's rays: tmin = 0, tmax = +inf).
+ * Hits are 4 words (int32 id, float t, float alpha, float beta), id -1 = miss.
+ */
+#ifndef ENCORE_ORACLE_H
+#define ENCORE_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct eo_hit {
+  int32_t id;
+  float t, alpha, beta;
+} eo_hit;
+
+/* TrianglePrim::intersect (TrianglePrim.cpp:204-248), FP32, clamp = apply
+ * ClampfloatoZero to the Cross() results (Vector3.h:148-161). */
+int eo_tri_test(const float* tri9, const float* ray8, int clamp, float* t, float* alpha,
+                float* beta);
+
+/* Brute-force closest hit over all triangles in ID order, strict-less
+ * replacement (BasicAS::intersect, BasicAS.cpp:167-194). */
+void eo_closest_brute(const float* tris, int ntris, const float* rays, long n, int clamp,
+                      eo_hit* out, int nthreads);
+/* Any hit with tmin < t < tmax (PhotonMapperCPU::IsInShadow's boolean). */
+void eo_occluded_brute(const float* tris, int ntris, const float* rays, long n, int clamp,
+                       uint8_t* out, int nthreads);
+/* Geometric truth: Moller-Trumbore in FP64, no clamp; t, alpha, beta rounded
+ * to float on output. */
+void eo_closest_f64(const float* tris, int ntris, const float* rays, long n, eo_hit* out,
+                    int nthreads);
+
+/* Geometric test of ray i against triangle ids[i] (FP64, no clamp): hit[i] = 1
+ * iff tmin < t < tmax; t[i] = FP64 distance.  Used to classify mismatches. */
+void eo_pairs_f64(const float* tris, const float* rays, const int32_t* ids, long n, uint8_t* hit,
+                  double* t);
+
+/* The reference kd-tree (Kdtree.cpp:84-200, 299-680) and its walk
+ * (Kdtree.cpp:682-784). */
+void* eo_kd_build(const float* tris, int ntris, int* max_depth, long* nnodes, long* nitems);
+void eo_kd_closest(void* kd, const float* rays, long n, int clamp, eo_hit* out, int nthreads);
+void eo_kd_free(void* kd);
+
+/* Photon gather: the k nearest accepted photons within max_dist
+ * (PhotonMap::GetNearestNPhotons, PhotonMap.cpp:76-94, 224-297: accept
+ * iff FP32 dist^2 < max_dist^2 and the stored normal equals the query
+ * normal unless ignore_normal) and the radiance estimate
+ * (GetRadianceEstimate, PhotonMap.cpp:121-164) accumulated in FP64.
+ * idx/d2 (k per query, ascending d2, -1 padded) and count may be NULL. */
+void* eo_pmap_build(const float* pos, const float* nrm, const float* power, long n);
+void eo_pmap_gather(void* pm, const float* qpos, const float* qnrm, long nq, int k,
+                    float max_dist, int ignore_normal, int caustic, double* rgb, int32_t* idx,
+                    float* d2, int32_t* count, int nthreads);
+void eo_pmap_free(void* pm);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every symbol include/encore_b200.h
+declares (no compute calls: these run without a GPU)."""
+import re
+from pathlib import Path
+
+from encore_b200 import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "encore_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:enc_status|int32_t|const char\*)\s+(enc_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "enc_accel_build" in syms and "enc_intersect_closest" in syms
+    assert "enc_photonmap_radiance" in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    assert set(declared_symbols()) <= set(_lib.SIGNATURES)
+
+
+def test_abi_version():
+    assert _lib.load().enc_abi_version() == 1
+
+
+def test_errors_without_device_are_reported_not_raised():
+    import ctypes as C
+    lib = _lib.load()
+    s = C.c_void_p()
+    assert lib.enc_scene_create(None, 0, C.byref(s)) == _lib.ENC_OK
+    a = C.c_void_p()
+    # empty scene is rejected before any device call
+    assert lib.enc_accel_build(s, None, 0, C.byref(a)) == _lib.ENC_ERR_INVALID_ARG
+    assert b"no triangles" in lib.enc_last_error()
+    lib.enc_scene_destroy(s)
+    assert lib.enc_accel_build(None, None, 0, C.byref(a)) == _lib.ENC_ERR_INVALID_ARG

@@ -1,0 +1,228 @@
+"""Parity of the CUDA traversal kernels with the reference (GPU).
+
+Bars: hit triangle IDs and any-hit booleans bit-exact, every mismatch on a
+near-tie or grazing hit listed and classified; t, alpha and beta bit-exact
+whenever the IDs agree (the predicate is the reference's FP32 operation
+order), which is inside the stated 1e-5 relative bound for t.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from encore_b200 import Accelerator, EncoreError, LaunchConfig, scenes
+from oracle import bindings as ob
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+T_RTOL = 1e-5
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.int32)
+
+
+def assert_same_where_ids_agree(got, want):
+    m = (got["tri"] == want["tri"]) & (want["tri"] >= 0)
+    assert np.array_equal(bits(got["t"][m]), bits(want["t"][m]))
+    assert np.array_equal(bits(got["u"][m]), bits(want["u"][m]))
+    assert np.array_equal(bits(got["v"][m]), bits(want["v"][m]))
+    np.testing.assert_allclose(got["t"][m], want["t"][m], rtol=T_RTOL)
+
+
+def assert_predicate_valid(tris, rays, got):
+    """Every reported hit is accepted by the oracle's FP32 reference predicate
+    with the same t/alpha/beta bits."""
+    h = got["tri"] >= 0
+    acc, t, a, b = ob.tri_test(tris, rays[h], got["tri"][h], clamp=True)
+    assert acc.all()
+    assert np.array_equal(bits(t), bits(got["t"][h]))
+    assert np.array_equal(bits(a), bits(got["u"][h]))
+    assert np.array_equal(bits(b), bits(got["v"][h]))
+
+
+@pytest.mark.parametrize("width", [2, 4, 8])
+@pytest.mark.parametrize("name", ["random2k_x1000.npz", "heightfield64_x1000.npz"])
+def test_wbvh_matches_reference_kdtree_golden_x1000(gpu, name, width):
+    g = np.load(GOLD / name)
+    want = np.zeros(len(g["rays"]), ob.HIT)
+    want["tri"], want["t"], want["u"], want["v"] = g["kd_tri"], g["kd_t"], g["kd_u"], g["kd_v"]
+    acc = Accelerator("wbvh", width=width).build(g["tris"])
+    got = acc.intersect(g["rays"])
+    mism, classes = ob.classify(g["tris"], g["rays"], got, want)
+    assert "unexplained" not in classes, list(zip(mism.tolist(), classes))
+    assert len(mism) <= max(2, len(want) // 1000), (len(mism), classes)
+    assert_same_where_ids_agree(got, want)
+    assert_predicate_valid(g["tris"], g["rays"], got)
+
+
+@pytest.mark.parametrize("name", ["random2k_x1.npz", "random2k_x1000.npz", "heightfield64_x1000.npz"])
+def test_kdtree_mode_bit_exact_with_reference(gpu, name):
+    """The flattened reference kd-tree walked on the GPU reproduces the
+    reference Kdtree exactly at every scale, clamp artefacts included."""
+    g = np.load(GOLD / name)
+    acc = Accelerator("kdtree").build(g["tris"])
+    got = acc.intersect(g["rays"])
+    assert np.array_equal(got["tri"], g["kd_tri"])
+    m = g["kd_tri"] >= 0
+    assert np.array_equal(bits(got["t"][m]), bits(g["kd_t"][m]))
+    assert np.array_equal(bits(got["u"][m]), bits(g["kd_u"][m]))
+    assert np.array_equal(bits(got["v"][m]), bits(g["kd_v"][m]))
+
+
+def test_kdtree_mode_matches_port_on_fresh_scene(gpu):
+    for scale in (1.0, 1000.0):
+        tris = scenes.random_triangles(20000, seed=101, scale=scale)
+        rays = np.concatenate([
+            scenes.camera_rays(128, 128, eye=np.array([0.5, 0.5, -1.5]) * scale,
+                               look=np.array([0.5, 0.5, 0.5]) * scale),
+            scenes.random_sphere_rays(8000, seed=102, hi=(scale, scale, scale))])
+        want = ob.PortKd(tris).closest(rays, clamp=True)
+        got = Accelerator("kdtree").build(tris).intersect(rays)
+        assert np.array_equal(got["tri"], want["tri"])
+        assert_same_where_ids_agree(got, want)
+
+
+def test_wbvh_unit_scale_mismatches_are_all_classified(gpu):
+    """At unit scale the reference predicate's Cross() clamp accepts hits off
+    the triangle, so every accelerator's answer depends on which triangles it
+    tests.  Every difference from the reference Kdtree must be a tie or a
+    clamp false positive on one side."""
+    g = np.load(GOLD / "random2k_x1.npz")
+    want = np.zeros(len(g["rays"]), ob.HIT)
+    want["tri"], want["t"], want["u"], want["v"] = g["kd_tri"], g["kd_t"], g["kd_u"], g["kd_v"]
+    got = Accelerator("wbvh").build(g["tris"]).intersect(g["rays"])
+    mism, classes = ob.classify(g["tris"], g["rays"], got, want)
+    assert "unexplained" not in classes, list(zip(mism.tolist(), classes))
+    assert_same_where_ids_agree(got, want)
+    assert_predicate_valid(g["tris"], g["rays"], got)
+
+
+@pytest.mark.parametrize("width", [2, 4, 8])
+def test_wbvh_matches_brute_force_x1000_fresh(gpu, width):
+    scale = 1000.0
+    tris = scenes.random_triangles(5000, seed=201, scale=scale)
+    rays = np.concatenate([
+        scenes.camera_rays(96, 96, eye=np.array([0.5, 0.5, -1.5]) * scale,
+                           look=np.array([0.5, 0.5, 0.5]) * scale),
+        scenes.random_sphere_rays(6000, seed=202, hi=(scale, scale, scale))])
+    want = ob.port_brute(tris, rays, clamp=True)
+    got = Accelerator("wbvh", width=width).build(tris).intersect(rays)
+    mism, classes = ob.classify(tris, rays, got, want)
+    assert "unexplained" not in classes
+    assert len(mism) <= 3
+    assert_same_where_ids_agree(got, want)
+
+
+def test_any_hit_matches_reference_golden(gpu):
+    g = np.load(GOLD / "random2k_x1000.npz")
+    for kind in ("wbvh", "kdtree"):
+        occ = Accelerator(kind).build(g["tris"]).occluded(g["shadow_rays"])
+        assert np.array_equal(occ, g["kd_occluded"]), kind
+
+
+def test_any_hit_matches_brute_force_fresh(gpu):
+    scale = 1000.0
+    tris = scenes.heightfield(res=48, seed=301, scale=scale)
+    pts = np.random.default_rng(302).random((6000, 3)).astype(np.float32) * scale
+    pts[:, 1] *= 0.3
+    sh = scenes.shadow_rays(pts, seed=303, light_center=np.array([0.5, 2.0, 0.5]) * scale,
+                            light_size=0.1 * scale, offset=0.01 * scale)
+    want = ob.port_occluded(tris, sh, clamp=True)
+    for width in (2, 4, 8):
+        got = Accelerator("wbvh", width=width).build(tris).occluded(sh)
+        assert np.array_equal(got, want), width
+
+
+def test_noclamp_predicate_matches_brute_force(gpu):
+    tris = scenes.random_triangles(3000, seed=401, scale=1.0)
+    rays = scenes.random_sphere_rays(5000, seed=402)
+    want = ob.port_brute(tris, rays, clamp=False)
+    got = Accelerator("wbvh", predicate="noclamp").build(tris).intersect(rays)
+    mism, classes = ob.classify(tris, rays, got, want)
+    assert len(mism) <= 3 and "unexplained" not in classes
+
+
+def test_tmin_tmax_window(gpu):
+    scale = 1000.0
+    tris = scenes.random_triangles(4000, seed=501, scale=scale)
+    rays = scenes.camera_rays(64, 64, eye=np.array([0.5, 0.5, -1.5]) * scale,
+                              look=np.array([0.5, 0.5, 0.5]) * scale)
+    rays[:, 3] = 1.9 * scale
+    rays[:, 7] = 2.1 * scale
+    want = ob.port_brute(tris, rays, clamp=True)
+    got = Accelerator("wbvh").build(tris).intersect(rays)
+    assert np.array_equal(got["tri"], want["tri"])
+    h = got["tri"] >= 0
+    assert np.all((got["t"][h] > 1.9 * scale) & (got["t"][h] < 2.1 * scale))
+
+
+def test_edge_cases(gpu):
+    tri = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32)
+    acc = Accelerator("wbvh").build(tri)
+    # empty batch
+    assert len(acc.intersect(np.zeros((0, 8), np.float32))) == 0
+    # axis-aligned directions with exact zeros; through, beside and behind
+    rays = np.array([
+        [0.25, 0.25, -1, 0, 0, 0, 1, np.inf],
+        [0.25, 0.25, 1, 0, 0, 0, -1, np.inf],
+        [2.0, 2.0, -1, 0, 0, 0, 1, np.inf],
+        [0.25, 0.25, 1, 0, 0, 0, 1, np.inf],   # pointing away
+        [-1, 0.25, 0, 0, 1, 0, 0, np.inf],     # in the plane (det = 0)
+    ], np.float32)
+    got = acc.intersect(rays)
+    want = ob.port_brute(tri, rays, clamp=True)
+    assert np.array_equal(got["tri"], want["tri"])
+    assert got["tri"].tolist() == [0, 0, -1, -1, -1]
+    kd = Accelerator("kdtree").build(tri).intersect(rays)
+    assert np.array_equal(kd["tri"], want["tri"])
+
+
+def test_launch_options_do_not_change_results(gpu):
+    scale = 1000.0
+    tris = scenes.heightfield(res=64, seed=601, scale=scale)
+    rays = scenes.random_sphere_rays(20000, seed=602, hi=(scale, 0.3 * scale, scale))
+    acc = Accelerator("wbvh").build(tris)
+    base = acc.intersect(rays)
+    for lc in (LaunchConfig(block_threads=32, blocks_per_sm=1, chunk=1, stack_depth=32),
+               LaunchConfig(block_threads=64, blocks_per_sm=8, chunk=256, stack_depth=64),
+               LaunchConfig(block_threads=128, blocks_per_sm=2, chunk=32, stack_depth=24)):
+        got = acc.intersect(rays, launch=lc)
+        assert np.array_equal(got["tri"], base["tri"])
+        assert np.array_equal(bits(got["t"]), bits(base["t"]))
+
+
+def test_stack_limit_is_reported_not_faulted(gpu):
+    """A stack too small for the tree stops the affected rays at the bound
+    and the call returns ENC_ERR_WATCHDOG; the context stays usable."""
+    scale = 1000.0
+    tris = scenes.random_triangles(50000, seed=701, scale=scale)
+    rays = scenes.random_sphere_rays(20000, seed=702, hi=(scale, scale, scale))
+    acc = Accelerator("wbvh", width=8).build(tris)
+    with pytest.raises(EncoreError) as ei:
+        acc.intersect(rays, launch=LaunchConfig(stack_depth=4))
+    assert ei.value.status == 4
+    got = acc.intersect(rays)  # still usable, default stack
+    want = ob.port_brute(tris, rays[:2000], clamp=True)
+    assert np.array_equal(got["tri"][:2000], want["tri"])
+
+
+def test_device_buffers_and_streams(gpu):
+    import torch
+    scale = 1000.0
+    tris = scenes.random_triangles(8000, seed=801, scale=scale)
+    rays = scenes.random_sphere_rays(30000, seed=802, hi=(scale, scale, scale))
+    acc = Accelerator("wbvh").build(tris)
+    host = acc.intersect(rays)
+    s = torch.cuda.Stream()
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((len(rays), 4), dtype=torch.int32, device="cuda")
+    d_occ = torch.empty(len(rays), dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(s):
+        acc.intersect_device(d_rays, len(rays), d_hits, stream=s)
+        acc.occluded_device(d_rays, len(rays), d_occ, stream=s)
+    acc.check(stream=s)
+    h = d_hits.cpu().numpy()
+    assert np.array_equal(h[:, 0], host["tri"])
+    assert np.array_equal(h[:, 1], host["t"].view(np.int32) * (host["tri"] >= 0))
+    assert np.array_equal(d_occ.cpu().numpy(), (host["tri"] >= 0).astype(np.uint8))
