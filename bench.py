@@ -90,58 +90,58 @@ def shadow_batch(tris, rays, hits, n: int, seed: int) -> np.ndarray:
 # clocks
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Polls the GPU's SM clock, power and clock-event reasons through NVML
+    every 2 ms from a background thread (the timed regions here last tens of
+    milliseconds, below nvidia-smi's sampling period)."""
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self.err = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: report that instead of a number
+            self.err = f"nvml unavailable: {e}"
+            return
+        reasons = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                   "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                   "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                   "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        def run():
+            while not self._stop.is_set():
+                try:
+                    sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                    pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, pw, [k for k, v in reasons.items() if r & v]))
+                except Exception as e:
+                    self.err = str(e)
+                    return
+                time.sleep(0.002)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, smax, reasons, power = [], [], set(), []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-                power.append(float(parts[3]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "power_w_max": max(power) if power else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "samples": 0,
+                    "reasons": [self.err or "no samples"]}
+        sm = [s[0] for s in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(min(sm)),
+                "sm_max_mhz": self.max_mhz, "power_w_max": max(s[1] for s in self.samples),
+                "samples": len(sm),
+                "reasons": sorted({r for s in self.samples for r in s[2]})}
 
 
 # ---------------------------------------------------------------------------

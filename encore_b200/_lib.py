@@ -95,7 +95,7 @@ def load(path: os.PathLike | None = None):
     with _lock:
         if _lib is not None:
             return _lib
-        p = Path(path) if path else LIB_PATH
+        p = Path(path or os.environ.get("ENC_LIB_PATH") or LIB_PATH)
         if not p.exists():
             raise RuntimeError(
                 f"{p} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "

@@ -3,6 +3,7 @@
 // AccelerationStructure / PhotonMap enters here.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -25,6 +26,9 @@ struct enc_accel_s {
   void* d_stage_in = nullptr;
   void* d_stage_out = nullptr;
   size_t stage_in_bytes = 0, stage_out_bytes = 0;
+  cudaStream_t pipe[2] = {nullptr, nullptr};  // host-form copy/trace pipeline
+  cudaEvent_t pipe_done[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_start = nullptr;
 };
 
 struct enc_photonmap_s {
@@ -125,9 +129,9 @@ Launch resolve_launch(const enc_launch_opts* o, int kind, int width) {
   (void)kind;
   Launch L;
   L.block = 128;
-  L.blocks_per_sm = width == 8 ? 4 : 4;
-  L.chunk = 64;
-  L.stack = 48;
+  L.blocks_per_sm = 8;
+  L.chunk = 32;
+  L.stack = 0;  // 0 = the tree's depth, which always suffices
   if (o) {
     if (o->block_threads > 0) L.block = o->block_threads;
     if (o->blocks_per_sm > 0) L.blocks_per_sm = o->blocks_per_sm;
@@ -236,6 +240,8 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
       WBVHHost h;
       build_wbvh(scene->verts.data(), scene->ntris, o.width, o.max_leaf_tris, &h);
       d.nnodes = h.nnodes;
+      d.tree_depth = h.depth;
+      if (h.depth > 64) throw std::runtime_error("wide BVH deeper than 64 levels");
       for (int i = 0; i < 3; ++i) {
         d.lo[i] = h.lo[i];
         d.hi[i] = h.hi[i];
@@ -278,8 +284,8 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
   }
   if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
   if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, 16);
-  if (e == cudaSuccess) e = cudaMemset(d.d_counter, 0, 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, kQueueSlots * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(d.d_counter, 0, kQueueSlots * sizeof(uint32_t));
   if (e != cudaSuccess) {
     free_dev(d);
     delete a;
@@ -297,6 +303,11 @@ enc_status enc_accel_destroy(enc_accel a) {
   free_dev(a->dev);
   cudaFree(a->d_stage_in);
   cudaFree(a->d_stage_out);
+  for (int i = 0; i < 2; ++i) {
+    if (a->pipe[i]) cudaStreamDestroy(a->pipe[i]);
+    if (a->pipe_done[i]) cudaEventDestroy(a->pipe_done[i]);
+  }
+  if (a->pipe_start) cudaEventDestroy(a->pipe_start);
   delete a;
   return ENC_OK;
 }
@@ -333,8 +344,8 @@ enc_status enc_intersect_closest_device(enc_accel a, const float* d_rays, size_t
   }
   DeviceScope ds(a->dev.device);
   Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
-  if (L.block % 32 != 0 || L.block > 128 || L.stack < 4 || L.stack > 64 || L.chunk < 1) {
-    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 4..64)");
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 0 or 2..64)");
     return ENC_ERR_INVALID_ARG;
   }
   int e = launch_closest(a->dev, d_rays, nrays, d_hits, L, stream, nullptr);
@@ -355,8 +366,8 @@ enc_status enc_intersect_any_device(enc_accel a, const float* d_rays, size_t nra
   }
   DeviceScope ds(a->dev.device);
   Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
-  if (L.block % 32 != 0 || L.block > 128 || L.stack < 4 || L.stack > 64 || L.chunk < 1) {
-    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 4..64)");
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 0 or 2..64)");
     return ENC_ERR_INVALID_ARG;
   }
   int e = launch_any(a->dev, d_rays, nrays, d_occ, L, stream);
@@ -364,49 +375,89 @@ enc_status enc_intersect_any_device(enc_accel a, const float* d_rays, size_t nra
   return ENC_OK;
 }
 
-enc_status enc_intersect_closest(enc_accel a, const float* rays, size_t nrays, enc_hit* hits,
-                                 const enc_launch_opts* launch, enc_stream stream) {
-  if (!a || (nrays && (!rays || !hits))) {
-    set_error("enc_intersect_closest: null argument");
+namespace {
+
+// Host-buffer form shared by closest and any hit.  Large batches are split
+// into chunks pipelined over two internal streams, so the copy of chunk i+1
+// in, the trace of chunk i and the copy of chunk i-1 out overlap (the copy
+// engines run both directions at once).  Ordering with the caller's stream
+// is kept with events; the call returns after the results are in `out`.
+enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, size_t out_bytes,
+                     bool any, const enc_launch_opts* launch, enc_stream stream, const char* what) {
+  if (!a || (nrays && (!rays || !out))) {
+    set_error(std::string(what) + ": null argument");
     return ENC_ERR_INVALID_ARG;
   }
   if (nrays == 0) return ENC_OK;
+  if (nrays > 0xffffffffull / 2) {
+    set_error(std::string(what) + ": too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 ||
+      L.chunk < 1) {
+    set_error(std::string(what) + ": launch options out of range");
+    return ENC_ERR_INVALID_ARG;
+  }
   std::lock_guard<std::mutex> lk(a->mu);
   DeviceScope ds(a->dev.device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   enc_status st = grow(&a->d_stage_in, &a->stage_in_bytes, nrays * 32);
   if (st) return st;
-  st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays * sizeof(enc_hit));
+  st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays * out_bytes);
   if (st) return st;
-  ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
-  st = enc_intersect_closest_device(a, (const float*)a->d_stage_in, nrays,
-                                    (enc_hit*)a->d_stage_out, launch, stream);
-  if (st) return st;
-  ENC_CUDA(cudaMemcpyAsync(hits, a->d_stage_out, nrays * sizeof(enc_hit), cudaMemcpyDeviceToHost, s),
-           "D2H hits");
+  if (!a->pipe[0]) {
+    for (int i = 0; i < 2; ++i) {
+      ENC_CUDA(cudaStreamCreateWithFlags(&a->pipe[i], cudaStreamNonBlocking), "stream create");
+      ENC_CUDA(cudaEventCreateWithFlags(&a->pipe_done[i], cudaEventDisableTiming), "event create");
+    }
+    ENC_CUDA(cudaEventCreateWithFlags(&a->pipe_start, cudaEventDisableTiming), "event create");
+  }
+  const size_t kChunk = (size_t)1 << 20;
+  const size_t nchunks = nrays <= 2 * kChunk ? 1 : (nrays + kChunk - 1) / kChunk;
+  const char* din = static_cast<const char*>(a->d_stage_in);
+  char* dout = static_cast<char*>(a->d_stage_out);
+  if (nchunks == 1) {
+    ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
+    int e = any ? launch_any(a->dev, (const float*)din, nrays, (uint8_t*)dout, L, s)
+                : launch_closest(a->dev, (const float*)din, nrays, (enc_hit*)dout, L, s, nullptr);
+    if (e) return cuda_fail((cudaError_t)e, "trace launch");
+    ENC_CUDA(cudaMemcpyAsync(out, dout, nrays * out_bytes, cudaMemcpyDeviceToHost, s), "D2H results");
+    return read_status(a, s);
+  }
+  ENC_CUDA(cudaEventRecord(a->pipe_start, s), "event record");
+  for (int i = 0; i < 2; ++i) ENC_CUDA(cudaStreamWaitEvent(a->pipe[i], a->pipe_start, 0), "wait");
+  for (size_t c = 0; c < nchunks; ++c) {
+    cudaStream_t ps = a->pipe[c & 1];
+    const size_t b = c * kChunk, n = std::min(kChunk, nrays - b);
+    ENC_CUDA(cudaMemcpyAsync((void*)(din + b * 32), rays + 8 * b, n * 32, cudaMemcpyHostToDevice, ps),
+             "H2D rays");
+    int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ps)
+                : launch_closest(a->dev, (const float*)(din + b * 32), n,
+                                 (enc_hit*)(dout + b * sizeof(enc_hit)), L, ps, nullptr);
+    if (e) return cuda_fail((cudaError_t)e, "trace launch");
+    ENC_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + b * out_bytes, dout + b * out_bytes,
+                             n * out_bytes, cudaMemcpyDeviceToHost, ps),
+             "D2H results");
+  }
+  for (int i = 0; i < 2; ++i) {
+    ENC_CUDA(cudaEventRecord(a->pipe_done[i], a->pipe[i]), "event record");
+    ENC_CUDA(cudaStreamWaitEvent(s, a->pipe_done[i], 0), "wait");
+  }
   return read_status(a, s);
+}
+
+}  // namespace
+
+enc_status enc_intersect_closest(enc_accel a, const float* rays, size_t nrays, enc_hit* hits,
+                                 const enc_launch_opts* launch, enc_stream stream) {
+  return host_form(a, rays, nrays, hits, sizeof(enc_hit), false, launch, stream,
+                   "enc_intersect_closest");
 }
 
 enc_status enc_intersect_any(enc_accel a, const float* rays, size_t nrays, uint8_t* occ,
                              const enc_launch_opts* launch, enc_stream stream) {
-  if (!a || (nrays && (!rays || !occ))) {
-    set_error("enc_intersect_any: null argument");
-    return ENC_ERR_INVALID_ARG;
-  }
-  if (nrays == 0) return ENC_OK;
-  std::lock_guard<std::mutex> lk(a->mu);
-  DeviceScope ds(a->dev.device);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  enc_status st = grow(&a->d_stage_in, &a->stage_in_bytes, nrays * 32);
-  if (st) return st;
-  st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays);
-  if (st) return st;
-  ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
-  st = enc_intersect_any_device(a, (const float*)a->d_stage_in, nrays, (uint8_t*)a->d_stage_out,
-                                launch, stream);
-  if (st) return st;
-  ENC_CUDA(cudaMemcpyAsync(occ, a->d_stage_out, nrays, cudaMemcpyDeviceToHost, s), "D2H occluded");
-  return read_status(a, s);
+  return host_form(a, rays, nrays, occ, 1, true, launch, stream, "enc_intersect_any");
 }
 
 enc_status enc_accel_check(enc_accel a, enc_stream stream) {

@@ -68,12 +68,14 @@ struct KdNode {
 
 // ---------------------------------------------------------------------------
 // Device-resident accelerator.
+constexpr int kQueueSlots = 256;
 struct DevAccel {
   int kind = 0;
   int width = 8;
   int predicate = 0;
   uint32_t ntris = 0;
   uint32_t nnodes = 0;
+  int tree_depth = 0;  // WBVH levels; the traversal stack needs at most depth - 1 entries
   // WBVH
   void* d_nodes = nullptr;      // nnodes * WNodeLayout<W>::kBytes
   DevTri* d_tris = nullptr;     // WBVH: leaf order; kd: triangle-ID order
@@ -84,7 +86,11 @@ struct DevAccel {
   float kd_root_lo[3] = {0, 0, 0}, kd_root_hi[3] = {0, 0, 0};
   // status word written by kernels (watchdog / bounds)
   uint32_t* d_status = nullptr;
-  uint32_t* d_counter = nullptr;  // work-queue heads (4 words)
+  // Work-queue heads: each launch takes the next of kQueueSlots words (and
+  // zeroes it on its stream), so up to kQueueSlots launches on one
+  // accelerator can be in flight on different streams.
+  uint32_t* d_counter = nullptr;
+  uint32_t counter_seq = 0;
   size_t node_bytes = 0, tri_bytes = 0, device_bytes = 0;
   int device = 0;
   double build_seconds = 0;
@@ -98,6 +104,7 @@ struct WBVHHost {
   uint32_t nnodes = 0;
   std::vector<DevTri> tris;    // leaf order
   float lo[3], hi[3];
+  int depth = 0;               // levels of wide nodes (root = 1)
 };
 
 struct KdHost {

@@ -4,8 +4,12 @@
 //    wide BVH.  Each warp takes rays from a global atomic queue in chunks and
 //    hands them to idle lanes as lanes finish (no lane waits for the slowest
 //    ray of a batch).  The traversal stack lives in shared memory, one column
-//    per thread.  Hit children of a node are ordered by entry distance with a
-//    sorting network; the nearest is visited next, the rest are pushed.
+//    per thread.  A visited node tests its triangles of hit leaves at once and
+//    continues with its first hit internal child; the others stay on the
+//    stack as one group entry.  Width 8 orders children by octant (the
+//    builder places each child in the slot of its octant, so slot k ^ octm
+//    for k = 0..7 is roughly front to back for a ray with direction sign
+//    bits octm); widths 2 and 4 sort hit children by entry distance.
 //  * kd_trace<CLAMP>: the reference's kd-tree walk (Kdtree.cpp:682-784), one
 //    thread per ray, over the flattened kd layout.  Bit-exact parity mode.
 //
@@ -24,6 +28,15 @@
 #include <cstdio>
 
 #include "engine.h"
+
+// Build-time tuning of the wide-BVH kernel:
+//   ENC_TRACE_MINBLOCKS resident 128-thread blocks per SM the register
+//                       budget is fitted to (8 -> 64 registers, no spills;
+//                       6 and 10 measured slower on the 2M-triangle
+//                       heightfield workload).
+#ifndef ENC_TRACE_MINBLOCKS
+#define ENC_TRACE_MINBLOCKS 8
+#endif
 
 namespace enc {
 namespace {
@@ -109,15 +122,18 @@ __device__ __forceinline__ uint32_t byte_of(const uint4* w, int off) {
   return (u[off >> 2] >> (8 * (off & 3))) & 0xffu;
 }
 
+// An 8-bit quantised coordinate as a float: the byte placed under the
+// exponent of 2^23 gives 2^23 + q exactly; subtracting 2^23 is exact.
+__device__ __forceinline__ float u8f(uint32_t q) {
+  return __uint_as_float(0x4B000000u | q) - 8388608.0f;
+}
+
 template <int W>
 struct NodeWords {
   static constexpr int N = WNodeLayout<W>::kBytes / 16;
   uint4 w[N];
 };
 
-// Item encoding on the stack: internal node index, or leaf with bit 31 set,
-// triangle count in bits 28..30 and first triangle in bits 0..27.
-constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kNoItem = 0xffffffffu;
 
 template <int W>
@@ -160,11 +176,22 @@ __device__ __forceinline__ void sort_net<8>(float (&k)[8], uint32_t (&v)[8]) {
 #undef ENC_CSWAP
 
 template <int W, bool CLAMP, bool ANY, bool COUNT>
-__global__ void __launch_bounds__(128) wbvh_trace(TraceParams P) {
+__global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TraceParams P) {
   using L = WNodeLayout<W>;
+  // Stack of node groups: one entry per visited node that still has hit
+  // internal children, so the depth never exceeds the tree depth.
+  //   W == 8: x = child_base, y = remaining hit children as bits k in
+  //           octant order (slot = k ^ octm) | internal-slot mask << 8;
+  //           lb = smallest entry distance among the group's hit children.
+  //   W < 8:  x = child_base, y = ranks of the remaining children sorted by
+  //           entry distance (3 bits each, nearest first) | count << 24;
+  //           lb = entry distance of the nearest remaining child.
+  // lb is a lower bound for every child still in the group, so a group
+  // whose lb exceeds the closest hit so far is dropped whole.
   extern __shared__ uint2 s_stack[];
   const int B = blockDim.x;
   uint2* stk = s_stack + threadIdx.x;  // entry i at stk[i * B]
+  float* slb = reinterpret_cast<float*>(s_stack + (size_t)P.stack_depth * B) + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = lanemask_lt();
 
@@ -177,7 +204,8 @@ __global__ void __launch_bounds__(128) wbvh_trace(TraceParams P) {
   float best_t = 0, bu = 0, bv = 0;
   int best_id = -1;
   int sp = 0;
-  uint32_t item = kNoItem;
+  uint32_t node = kNoItem;
+  uint32_t octm = 0;  // direction sign bits: bit a set = negative along axis a
   unsigned steps = 0;
   uint32_t nvis = 0, ntest = 0;
 
@@ -204,10 +232,18 @@ __global__ void __launch_bounds__(128) wbvh_trace(TraceParams P) {
         const float4 r1 = __ldg(P.rays + 2 * (size_t)ray + 1);
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
-        ix = 1.0f / dx; iy = 1.0f / dy; iz = 1.0f / dz;
+        // Box tests use a reciprocal with |d| floored at 1e-20 so that a zero
+        // direction component (the reference's Normalize clamps small ones to
+        // exactly 0) gives finite slab distances instead of 0 * inf = NaN,
+        // which would leave that axis unconstrained.  The triangle predicate
+        // keeps the exact direction.
+        ix = 1.0f / (fabsf(dx) > 1e-20f ? dx : copysignf(1e-20f, dx));
+        iy = 1.0f / (fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy));
+        iz = 1.0f / (fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz));
+        octm = (dx < 0.f ? 1u : 0u) | (dy < 0.f ? 2u : 0u) | (dz < 0.f ? 4u : 0u);
         best_t = tmax; best_id = -1; bu = 0.f; bv = 0.f;
         sp = 0;
-        item = 0;  // root
+        node = 0;  // root
         steps = 0;
         nvis = 0; ntest = 0;
       }
@@ -220,126 +256,219 @@ __global__ void __launch_bounds__(128) wbvh_trace(TraceParams P) {
     if (ray >= 0) {
       bool done = false;
       bool hit_any = false;
-      ++steps;
-      if (steps > kMaxSteps) {
+      if (++steps > kMaxSteps) {
         atomicOr(P.status, kStatusWatchdog);
         best_id = -1;
         done = true;
-      } else if (!(item & kLeafBit)) {
-        // ---- internal node: test all children ---------------------------
-        if (item >= P.nnodes) {
-          atomicOr(P.status, kStatusBounds);
-          best_id = -1;
-          done = true;
-        } else {
-          if (COUNT) ++nvis;
-          NodeWords<W> nw;
-          const uint4* src = reinterpret_cast<const uint4*>(P.nodes + (size_t)item * L::kBytes);
+      } else if (node >= P.nnodes) {
+        atomicOr(P.status, kStatusBounds);
+        best_id = -1;
+        done = true;
+      } else {
+        // ---- visit one node: its hit leaves now, its hit internal children
+        //      in front-to-back order (one continues, the rest become one
+        //      group on the stack) ------------------------------------------
+        if (COUNT) ++nvis;
+        NodeWords<W> nw;
+        const uint4* src = reinterpret_cast<const uint4*>(P.nodes + (size_t)node * L::kBytes);
 #pragma unroll
-          for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = __ldg(src + i);
-          const float px = __uint_as_float(nw.w[0].x);
-          const float py = __uint_as_float(nw.w[0].y);
-          const float pz = __uint_as_float(nw.w[0].z);
-          const uint32_t ew = nw.w[0].w;
-          const float sx = __uint_as_float((ew & 0xffu) << 23);
-          const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
-          const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
-          const uint32_t child_base = nw.w[1].x;
-          const uint32_t tri_base = nw.w[1].y;
-          const float bx = (px - ox) * ix, by = (py - oy) * iy, bz = (pz - oz) * iz;
-          const float cx = sx * ix, cy = sy * iy, cz = sz * iz;
-          float key[W];
-          uint32_t val[W];
-          int nh = 0;
+        for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = __ldg(src + i);
+        const float px = __uint_as_float(nw.w[0].x);
+        const float py = __uint_as_float(nw.w[0].y);
+        const float pz = __uint_as_float(nw.w[0].z);
+        const uint32_t ew = nw.w[0].w;
+        const float sx = __uint_as_float((ew & 0xffu) << 23);
+        const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
+        const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
+        const uint32_t child_base = nw.w[1].x;
+        const uint32_t tri_base = nw.w[1].y;
+        const float bx = (px - ox) * ix, by = (py - oy) * iy, bz = (pz - oz) * iz;
+        const float cx = sx * ix, cy = sy * iy, cz = sz * iz;
+        // Near and far planes per axis by the ray's direction sign: the
+        // near plane of a child box is its lo corner for a positive
+        // direction and its hi corner for a negative one.
+        const bool nxs = (octm & 1u) != 0, nys = (octm & 2u) != 0, nzs = (octm & 4u) != 0;
+        float key[W];
+        uint32_t rnk[W];
+        uint32_t trimask = 0;
+        uint32_t hitk = 0;      // W == 8: hit internal children, bit k = slot k ^ octm
+        float lbmin = INFINITY;  // W == 8: smallest entry distance of those
+        int nh = 0;
+        // Width 8: the six plane arrays are whole words (qlo x at words 8-9,
+        // y 10-11, z 12-13, qhi x 14-15, y 16-17, z 18-19), so near/far are
+        // chosen once per word and each byte becomes 2^23 + q with one PRMT.
+        uint32_t wn[6], wf[6];
+        if constexpr (W == 8) {
+          const uint32_t* u = reinterpret_cast<const uint32_t*>(nw.w);
+          const bool neg[3] = {nxs, nys, nzs};
 #pragma unroll
-          for (int c = 0; c < W; ++c) {
-            const float qlx = (float)byte_of(nw.w, L::kQOff + 0 * W + c);
-            const float qly = (float)byte_of(nw.w, L::kQOff + 1 * W + c);
-            const float qlz = (float)byte_of(nw.w, L::kQOff + 2 * W + c);
-            const float qhx = (float)byte_of(nw.w, L::kQOff + 3 * W + c);
-            const float qhy = (float)byte_of(nw.w, L::kQOff + 4 * W + c);
-            const float qhz = (float)byte_of(nw.w, L::kQOff + 5 * W + c);
-            const float t0x = fmaf(qlx, cx, bx), t1x = fmaf(qhx, cx, bx);
-            const float t0y = fmaf(qly, cy, by), t1y = fmaf(qhy, cy, by);
-            const float t0z = fmaf(qlz, cz, bz), t1z = fmaf(qhz, cz, bz);
-            const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
-            const float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
-            const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
-            const bool hit = meta != 0u && tn <= tf;
-            uint32_t it;
-            if (meta >= 32u)
-              it = kLeafBit | ((meta >> 5) << 28) | (tri_base + (meta & 31u));
-            else
-              it = child_base + meta - 1u;
-            key[c] = hit ? fminf(tn, 3.0e38f) : INFINITY;  // hits sort before empty slots
-            val[c] = it;
-            nh += hit ? 1 : 0;
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const uint32_t lo = u[8 + 2 * a + h], hi = u[14 + 2 * a + h];
+              wn[2 * a + h] = neg[a] ? hi : lo;
+              wf[2 * a + h] = neg[a] ? lo : hi;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+          float tnx, tfx, tny, tfy, tnz, tfz;
+          if constexpr (W == 8) {
+            const uint32_t sel = 0x7650u | (uint32_t)(c & 3);
+            const int h = c >> 2;
+            tnx = fmaf(__uint_as_float(__byte_perm(wn[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
+            tfx = fmaf(__uint_as_float(__byte_perm(wf[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
+            tny = fmaf(__uint_as_float(__byte_perm(wn[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
+            tfy = fmaf(__uint_as_float(__byte_perm(wf[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
+            tnz = fmaf(__uint_as_float(__byte_perm(wn[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
+            tfz = fmaf(__uint_as_float(__byte_perm(wf[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
+          } else {
+            const uint32_t qlx = byte_of(nw.w, L::kQOff + 0 * W + c);
+            const uint32_t qly = byte_of(nw.w, L::kQOff + 1 * W + c);
+            const uint32_t qlz = byte_of(nw.w, L::kQOff + 2 * W + c);
+            const uint32_t qhx = byte_of(nw.w, L::kQOff + 3 * W + c);
+            const uint32_t qhy = byte_of(nw.w, L::kQOff + 4 * W + c);
+            const uint32_t qhz = byte_of(nw.w, L::kQOff + 5 * W + c);
+            tnx = fmaf(u8f(nxs ? qhx : qlx), cx, bx);
+            tfx = fmaf(u8f(nxs ? qlx : qhx), cx, bx);
+            tny = fmaf(u8f(nys ? qhy : qly), cy, by);
+            tfy = fmaf(u8f(nys ? qly : qhy), cy, by);
+            tnz = fmaf(u8f(nzs ? qhz : qlz), cz, bz);
+            tfz = fmaf(u8f(nzs ? qlz : qhz), cz, bz);
           }
-          if (nh > 0) {
-            sort_net<W>(key, val);
-            if (sp + nh - 1 > P.stack_depth) {
-              atomicOr(P.status, kStatusStack);
-              best_id = -1;
-              done = true;
-            } else {
-              // push hits 1..nh-1 farthest first
-#pragma unroll
-              for (int c = W - 1; c >= 1; --c) {
-                if (c < nh) {
-                  stk[(sp + (nh - 1 - c)) * B] = make_uint2(val[c], __float_as_uint(key[c]));
-                }
-              }
-              sp += nh - 1;
-              item = val[0];
+          const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+          const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+          const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
+          const bool hit = meta != 0u && tn <= tf;
+          const bool leaf = meta >= 32u;
+          if (hit && leaf) trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+          const bool ih = hit && !leaf;
+          if constexpr (W == 8) {
+            if (ih) {
+              hitk |= 1u << ((uint32_t)c ^ octm);
+              lbmin = fminf(lbmin, tn);
             }
           } else {
-            item = kNoItem;
+            key[c] = ih ? fminf(tn, 3.0e38f) : INFINITY;  // hits sort before the rest
+            rnk[c] = meta - 1u;
+            nh += ih ? 1 : 0;
           }
         }
-      } else {
-        // ---- leaf: test its triangles ----------------------------------
-        const uint32_t first = item & 0x0fffffffu;
-        const uint32_t cnt = (item >> 28) & 7u;
-        if (first + cnt > P.ntris) {
-          atomicOr(P.status, kStatusBounds);
-          best_id = -1;
-          done = true;
-        } else {
-          for (uint32_t k = 0; k < cnt; ++k) {
-            const float4* tp = P.tris + 3 * (size_t)(first + k);
-            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            if (COUNT) ++ntest;
-            float t, u, v;
-            if (tri_test<CLAMP>(a, b, c, ox, oy, oz, dx, dy, dz, tmin, t, u, v)) {
-              const int id = __float_as_int(c.y);
-              if (ANY) {
-                if (t < tmax) {
-                  hit_any = true;
-                  break;
-                }
-              } else if (t < best_t || (t == best_t && id < best_id)) {
-                best_t = t;
-                best_id = id;
-                bu = u;
-                bv = v;
+        // ---- next node, and the group of the other hit children ----------
+        if constexpr (W == 8) {
+          if (hitk) {
+            // internal-child mask in slot order, for ranks within child_base
+            uint32_t imask = 0;
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+              const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
+              imask |= (meta != 0u && meta < 32u) ? (1u << c) : 0u;
+            }
+            const uint32_t k = __ffs(hitk) - 1;
+            const uint32_t slot = k ^ octm;
+            node = child_base + __popc(imask & ((1u << slot) - 1u));
+            const uint32_t rest = hitk & (hitk - 1u);
+            if (rest) {
+              if (sp >= P.stack_depth) {
+                atomicOr(P.status, kStatusStack);
+                best_id = -1;
+                done = true;
+              } else {
+                stk[sp * B] = make_uint2(child_base, rest | (imask << 8));
+                slb[sp * B] = lbmin;
+                ++sp;
               }
             }
+          } else {
+            node = kNoItem;
           }
-          item = kNoItem;
+        } else {
+          if (nh > 0) {
+            sort_net<W>(key, rnk);
+            node = child_base + rnk[0];
+            if (nh > 1) {
+              if (sp >= P.stack_depth) {
+                atomicOr(P.status, kStatusStack);
+                best_id = -1;
+                done = true;
+              } else {
+                uint32_t packed = 0;
+#pragma unroll
+                for (int c = W - 1; c >= 1; --c)
+                  if (c < nh) packed = (packed << 3) | (rnk[c] & 7u);
+                stk[sp * B] = make_uint2(child_base, packed | ((uint32_t)(nh - 1) << 24));
+                slb[sp * B] = key[1];
+                ++sp;
+              }
+            }
+          } else {
+            node = kNoItem;
+          }
+        }
+        // ---- triangles of the hit leaves ---------------------------------
+        while (trimask) {
+          const uint32_t k = __ffs(trimask) - 1;
+          trimask &= trimask - 1;
+          const uint32_t ti = tri_base + k;
+          if (ti >= P.ntris) {
+            atomicOr(P.status, kStatusBounds);
+            continue;
+          }
+          const float4* tp = P.tris + 3 * (size_t)ti;
+          const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+          if (COUNT) ++ntest;
+          float t, u, v;
+          if (tri_test<CLAMP>(a, b, c, ox, oy, oz, dx, dy, dz, tmin, t, u, v)) {
+            const int id = __float_as_int(c.y);
+            if (ANY) {
+              if (t < tmax) {
+                hit_any = true;
+                break;
+              }
+            } else if (t < best_t || (t == best_t && id < best_id)) {
+              best_t = t;
+              best_id = id;
+              bu = u;
+              bv = v;
+            }
+          }
         }
         if (ANY && hit_any) done = true;
       }
-      // ---- pop the next item whose entry distance can still matter ------
-      if (!done && item == kNoItem) {
+      // ---- pop the next group child that can still matter ----------------
+      if (!done && node == kNoItem) {
         while (sp > 0) {
-          const uint2 e = stk[(sp - 1) * B];
-          --sp;
-          if (ANY || __uint_as_float(e.y) <= best_t) {
-            item = e.x;
-            break;
+          if (!ANY && slb[(sp - 1) * B] > best_t) {
+            --sp;
+            continue;
           }
+          uint2 e = stk[(sp - 1) * B];
+          if constexpr (W == 8) {
+            const uint32_t hk = e.y & 0xffu;
+            const uint32_t k = __ffs(hk) - 1;
+            const uint32_t slot = k ^ octm;
+            const uint32_t imask = (e.y >> 8) & 0xffu;
+            node = e.x + __popc(imask & ((1u << slot) - 1u));
+            const uint32_t rest = hk & (hk - 1u);
+            if (rest == 0) {
+              --sp;
+            } else {
+              e.y = rest | (imask << 8);
+              stk[(sp - 1) * B] = e;
+            }
+          } else {
+            const uint32_t cnt = e.y >> 24;
+            node = e.x + (e.y & 7u);
+            if (cnt <= 1) {
+              --sp;
+            } else {
+              e.y = (((e.y & 0xffffffu) >> 3)) | ((cnt - 1) << 24);
+              stk[(sp - 1) * B] = e;
+            }
+          }
+          break;
         }
-        if (item == kNoItem) done = true;
+        if (node == kNoItem) done = true;
       }
       if (done) {
         if (ANY) {
@@ -357,7 +486,7 @@ __global__ void __launch_bounds__(128) wbvh_trace(TraceParams P) {
           P.visits[2 * (size_t)ray + 1] = ntest;
         }
         ray = -1;
-        item = kNoItem;
+        node = kNoItem;
       }
     }
   }
@@ -514,20 +643,24 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
   p.rays = reinterpret_cast<const float4*>(rays);
   p.out = out;
   p.visits = visits;
-  p.counter = a.d_counter;
+  const uint32_t slot =
+      __atomic_fetch_add(const_cast<uint32_t*>(&a.counter_seq), 1u, __ATOMIC_RELAXED) % kQueueSlots;
+  p.counter = a.d_counter + slot;
   p.status = a.d_status;
   p.nrays = (unsigned)n;
   p.nnodes = a.nnodes;
   p.ntris = a.ntris;
-  p.stack_depth = L.stack;
+  // Each visited node leaves at most one group entry, so tree_depth - 1
+  // entries always suffice; 0 selects that bound.
+  p.stack_depth = L.stack > 0 ? L.stack : (a.tree_depth > 8 ? a.tree_depth : 8);
   p.chunk = L.chunk;
-  size_t smem = (size_t)L.stack * L.block * sizeof(uint2);
+  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
   auto k = wbvh_trace<W, CLAMP, ANY, COUNT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
   }
-  cudaError_t e = cudaMemsetAsync(a.d_counter, 0, sizeof(unsigned), s);
+  cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return (int)e;
   int grid = device_sm_count(a.device) * L.blocks_per_sm;
   k<<<grid, L.block, smem, s>>>(p);

@@ -198,7 +198,10 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
               const float* tri_verts, WBVHHost* out) {
   using L = WNodeLayout<W>;
   std::vector<uint32_t> queue;  // binary node per wide node, BFS order
+  std::vector<uint16_t> level;  // depth of each wide node (root = 1)
   queue.push_back(0);
+  level.push_back(1);
+  int max_level = 1;
   std::vector<uint8_t>& nodes = out->nodes;
   std::vector<uint32_t> tri_order;
   tri_order.reserve(order.size());
@@ -251,18 +254,66 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
     h.nchild = (uint8_t)nk;
     h.child_base = (uint32_t)(queue.size());
     h.tri_base = (uint32_t)tri_order.size();
+    // Slot order.  Width 8: slot s holds the child lying most in octant s
+    // (bit a of s set = positive side of axis a) relative to the node centre,
+    // assigned greedily by largest dot(child centre - node centre, octant
+    // direction).  A ray whose direction is negative on the axes in mask m
+    // then meets the children roughly front to back in slot order k ^ m,
+    // k = 0..7, with no per-node sort.  Widths 2 and 4 keep build order.
+    int slot_child[W];
+    for (int s = 0; s < W; ++s) slot_child[s] = -1;
+    if (W == 8) {
+      float ctr[3];
+      for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
+      float score[8][8];
+      for (int i = 0; i < nk; ++i) {
+        const Box& cb = bn[kids[i]].box;
+        float d[3];
+        for (int a = 0; a < 3; ++a) d[a] = 0.5f * (cb.lo[a] + cb.hi[a]) - ctr[a];
+        for (int s = 0; s < 8; ++s)
+          score[i][s] = ((s & 1) ? d[0] : -d[0]) + ((s & 2) ? d[1] : -d[1]) + ((s & 4) ? d[2] : -d[2]);
+      }
+      bool used_child[8] = {false}, used_slot[8] = {false};
+      for (int it = 0; it < nk; ++it) {
+        int bi = -1, bs = -1;
+        float bv = -INFINITY;
+        for (int i = 0; i < nk; ++i)
+          if (!used_child[i])
+            for (int s = 0; s < 8; ++s)
+              if (!used_slot[s] && (bi < 0 || score[i][s] > bv)) {
+                bv = score[i][s];
+                bi = i;
+                bs = s;
+              }
+        used_child[bi] = true;
+        used_slot[bs] = true;
+        slot_child[bs] = bi;
+      }
+    } else {
+      for (int i = 0; i < nk; ++i) slot_child[i] = i;
+    }
     int n_internal = 0;
     uint8_t* meta = raw.data() + L::kMetaOff;
     uint8_t* q = raw.data() + L::kQOff;
-    for (int i = 0; i < nk; ++i) {
-      const BNode& c = bn[kids[i]];
+    for (int i = 0; i < W; ++i) {
+      if (slot_child[i] < 0) {
+        // Empty slot: meta 0 and an inverted box (lo 255, hi 0), never hit.
+        for (int a = 0; a < 3; ++a) {
+          q[a * W + i] = 255;
+          q[(3 + a) * W + i] = 0;
+        }
+        continue;
+      }
+      const BNode& c = bn[kids[slot_child[i]]];
       if (c.left >= 0) {
         meta[i] = (uint8_t)(1 + n_internal);
         ++n_internal;
-        queue.push_back(kids[i]);
+        queue.push_back(kids[slot_child[i]]);
+        level.push_back((uint16_t)(level[qi] + 1));
+        max_level = std::max(max_level, (int)level[qi] + 1);
       } else {
         uint32_t off = (uint32_t)tri_order.size() - h.tri_base;
-        if (c.count < 1 || c.count > 7 || off > 31)
+        if (c.count < 1 || c.count > 7 || off + c.count > 32)
           throw std::runtime_error("leaf packing overflow");
         meta[i] = (uint8_t)((c.count << 5) | off);
         for (uint32_t k = 0; k < c.count; ++k) tri_order.push_back(order[c.first + k]);
@@ -276,16 +327,11 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
         q[(3 + a) * W + i] = (uint8_t)hi;
       }
     }
-    // Empty slots: an inverted box (lo 255, hi 0) never produces a hit.
-    for (int i = nk; i < W; ++i)
-      for (int a = 0; a < 3; ++a) {
-        q[a * W + i] = 255;
-        q[(3 + a) * W + i] = 0;
-      }
     std::memcpy(raw.data(), &h, sizeof(h));
     nodes.insert(nodes.end(), raw.begin(), raw.end());
   }
   out->nnodes = (uint32_t)queue.size();
+  out->depth = max_level;
   out->tris.resize(tri_order.size());
   make_dev_tris(tri_verts, (uint32_t)tri_order.size(), tri_order.data(), out->tris.data());
 }

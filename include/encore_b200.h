@@ -96,7 +96,8 @@ typedef struct enc_launch_opts {
   int32_t block_threads; /* threads per block, multiple of 32 (0 = tuned default) */
   int32_t blocks_per_sm; /* persistent CTAs per SM (0 = tuned default) */
   int32_t chunk;         /* rays a warp takes from the queue per refill (0 = 32) */
-  int32_t stack_depth;   /* traversal stack entries per ray (0 = 32; max 64) */
+  int32_t stack_depth;   /* traversal stack entries per ray (0 = the tree depth, which
+                            always suffices; max 64) */
 } enc_launch_opts;
 
 typedef struct enc_accel_info {

@@ -50,8 +50,11 @@ def test_wbvh_matches_reference_kdtree_golden_x1000(gpu, name, width):
     acc = Accelerator("wbvh", width=width).build(g["tris"])
     got = acc.intersect(g["rays"])
     mism, classes = ob.classify(g["tris"], g["rays"], got, want)
+    # listed: ties on shared edges (equal FP32 t, the reference keeps the one
+    # its traversal meets first, the engine the lower ID)
     assert "unexplained" not in classes, list(zip(mism.tolist(), classes))
-    assert len(mism) <= max(2, len(want) // 1000), (len(mism), classes)
+    non_tie = [c for c in classes if c != "tie"]
+    assert len(non_tie) <= max(2, len(want) // 1000), (len(mism), classes)
     assert_same_where_ids_agree(got, want)
     assert_predicate_valid(g["tris"], g["rays"], got)
 
@@ -110,7 +113,7 @@ def test_wbvh_matches_brute_force_x1000_fresh(gpu, width):
     got = Accelerator("wbvh", width=width).build(tris).intersect(rays)
     mism, classes = ob.classify(tris, rays, got, want)
     assert "unexplained" not in classes
-    assert len(mism) <= 3
+    assert len([c for c in classes if c != "tie"]) <= 3
     assert_same_where_ids_agree(got, want)
 
 
@@ -200,7 +203,7 @@ def test_stack_limit_is_reported_not_faulted(gpu):
     rays = scenes.random_sphere_rays(20000, seed=702, hi=(scale, scale, scale))
     acc = Accelerator("wbvh", width=8).build(tris)
     with pytest.raises(EncoreError) as ei:
-        acc.intersect(rays, launch=LaunchConfig(stack_depth=4))
+        acc.intersect(rays, launch=LaunchConfig(stack_depth=2))
     assert ei.value.status == 4
     got = acc.intersect(rays)  # still usable, default stack
     want = ob.port_brute(tris, rays[:2000], clamp=True)
@@ -226,3 +229,26 @@ def test_device_buffers_and_streams(gpu):
     assert np.array_equal(h[:, 0], host["tri"])
     assert np.array_equal(h[:, 1], host["t"].view(np.int32) * (host["tri"] >= 0))
     assert np.array_equal(d_occ.cpu().numpy(), (host["tri"] >= 0).astype(np.uint8))
+
+
+def test_pipelined_host_form_matches_device_form(gpu):
+    """Batches above two chunks go through the copy/trace pipeline; results
+    must equal the single-launch device form bit for bit."""
+    import torch
+    scale = 1000.0
+    tris = scenes.random_triangles(20000, seed=901, scale=scale)
+    rays = scenes.random_sphere_rays(2_600_000, seed=902, hi=(scale, scale, scale))
+    acc = Accelerator("wbvh").build(tris)
+    host = acc.intersect(rays)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((len(rays), 4), dtype=torch.int32, device="cuda")
+    acc.intersect_device(d_rays, len(rays), d_hits)
+    acc.check()
+    dev = d_hits.cpu().numpy()
+    assert np.array_equal(dev[:, 0], host["tri"])
+    assert np.array_equal(dev[:, 1], host["t"].view(np.int32))
+    occ = acc.occluded(rays)
+    assert np.array_equal(occ, (host["tri"] >= 0).astype(np.uint8))
+    sub = np.arange(0, len(rays), 997)
+    want = ob.port_brute(tris, rays[sub], clamp=True)
+    assert np.array_equal(host["tri"][sub], want["tri"])
