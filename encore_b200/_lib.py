@@ -78,6 +78,7 @@ SIGNATURES = {
     "enc_intersect_any_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_accel_check": (C.c_int32, [P, P]),
     "enc_accel_count_visits": (C.c_int32, [P, P, C.c_size_t, P, P]),
+    "enc_intersect_closest_noalloc": (C.c_int32, [P, P, C.c_size_t, P, P]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),

@@ -125,6 +125,8 @@ enc_status read_status(enc_accel a, cudaStream_t s) {
 
 void set_error(const std::string& msg) { g_err = msg; }
 
+const DevAccel* accel_device_view(enc_accel a) { return a ? &a->dev : nullptr; }
+
 Launch resolve_launch(const enc_launch_opts* o, int kind, int width) {
   (void)kind;
   Launch L;

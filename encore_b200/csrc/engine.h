@@ -133,9 +133,17 @@ int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_
                    const Launch& L, void* stream, uint32_t* d_visits);
 int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
                const Launch& L, void* stream);
+// Wide-BVH closest hit whose queue head (*counter, zeroed by the caller on
+// `stream`) and status word are caller-provided device words.
+int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size_t n,
+                                    enc_hit* d_hits, const Launch& L, void* stream,
+                                    uint32_t* counter, uint32_t* status);
 int device_sm_count(int device);
 
 // Error reporting (capi.cpp).
 void set_error(const std::string& msg);
+
+// The device view of an accelerator handle, or nullptr (capi.cpp).
+const DevAccel* accel_device_view(enc_accel a);
 
 }  // namespace enc

@@ -743,4 +743,56 @@ int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
   return dispatch_w<true, false>(a, d_rays, n, d_occ, nullptr, L, s);
 }
 
+namespace {
+
+// Closest hit over the wide BVH with the queue head and status word supplied
+// by the caller instead of taken from the accelerator.
+template <int W, bool CLAMP>
+int launch_w_external(const DevAccel& a, const float* rays, size_t n, enc_hit* hits,
+                      const Launch& L, cudaStream_t s, uint32_t* counter, uint32_t* status) {
+  TraceParams p;
+  p.nodes = static_cast<const uint8_t*>(a.d_nodes);
+  p.tris = reinterpret_cast<const float4*>(a.d_tris);
+  p.rays = reinterpret_cast<const float4*>(rays);
+  p.out = hits;
+  p.visits = nullptr;
+  p.counter = counter;
+  p.status = status;
+  p.nrays = (unsigned)n;
+  p.nnodes = a.nnodes;
+  p.ntris = a.ntris;
+  p.stack_depth = L.stack > 0 ? L.stack : (a.tree_depth > 8 ? a.tree_depth : 8);
+  p.chunk = L.chunk;
+  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
+  auto k = wbvh_trace<W, CLAMP, false, false>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+  }
+  int grid = device_sm_count(a.device) * L.blocks_per_sm;
+  k<<<grid, L.block, smem, s>>>(p);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size_t n,
+                                    enc_hit* d_hits, const Launch& L, void* stream,
+                                    uint32_t* counter, uint32_t* status) {
+  if (n == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool clamp = a.predicate == ENC_PRED_REFERENCE;
+  switch (a.width) {
+    case 2:
+      return clamp ? launch_w_external<2, true>(a, d_rays, n, d_hits, L, s, counter, status)
+                   : launch_w_external<2, false>(a, d_rays, n, d_hits, L, s, counter, status);
+    case 4:
+      return clamp ? launch_w_external<4, true>(a, d_rays, n, d_hits, L, s, counter, status)
+                   : launch_w_external<4, false>(a, d_rays, n, d_hits, L, s, counter, status);
+    default:
+      return clamp ? launch_w_external<8, true>(a, d_rays, n, d_hits, L, s, counter, status)
+                   : launch_w_external<8, false>(a, d_rays, n, d_hits, L, s, counter, status);
+  }
+}
+
 }  // namespace enc

@@ -160,6 +160,22 @@ enc_status enc_accel_check(enc_accel accel, enc_stream stream);
 enc_status enc_accel_count_visits(enc_accel accel, const float* d_rays, size_t nrays,
                                   uint32_t* d_visits, enc_stream stream);
 
+/* Closest hit from host buffers with no device allocation.  This entry point
+ * has no counterpart in the reference.  It is for callers that must not call
+ * cudaMalloc/cudaFree while answering queries: code whose host framework
+ * already owns the device memory, or frame loops that cannot take the
+ * device-wide synchronisation an allocation can cause.  Results equal
+ * enc_intersect_closest's.  Scratch (rays in, hits out, queue head, status)
+ * is one fixed __device__ array inside this library, about 3 MiB per GPU that
+ * loads it, held until exit; a batch may hold at most ENC_NOALLOC_MAX_RAYS
+ * rays (more is ENC_ERR_INVALID_ARG).  The first call for a device looks up
+ * the array's device address; make it before any stream capture.  Calls
+ * share the array: calls from one process are serialised and synchronous,
+ * and calls that overlap on the GPU race.  Wide-BVH accelerators only. */
+#define ENC_NOALLOC_MAX_RAYS 65536
+enc_status enc_intersect_closest_noalloc(enc_accel accel, const float* rays, size_t nrays,
+                                         enc_hit* hits, enc_stream stream);
+
 /* PhotonMap: AddPhoton x n followed by BalanceAndConstruct
  * (PhotonMap.cpp:46-53, 167-221).  caustic != 0 selects the caustic-map
  * estimate (cone weight and N/(pi r^2), PhotonMap.cpp:147, 157). */
