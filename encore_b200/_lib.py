@@ -59,6 +59,11 @@ class AccelInfo(C.Structure):
                 ("scene_hi", C.c_float * 3)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("accel", C.c_void_p), ("d_rays", C.c_void_p), ("d_hits", C.c_void_p),
+                ("nrays", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 P = C.c_void_p
 F = C.POINTER(C.c_float)
 
@@ -79,6 +84,12 @@ SIGNATURES = {
     "enc_accel_check": (C.c_int32, [P, P]),
     "enc_accel_count_visits": (C.c_int32, [P, P, C.c_size_t, P, P]),
     "enc_intersect_closest_noalloc": (C.c_int32, [P, P, C.c_size_t, P, P]),
+    "enc_batch_create": (C.c_int32, [C.POINTER(BatchItem), C.c_uint32, C.POINTER(LaunchOpts),
+                                     C.POINTER(P)]),
+    "enc_batch_launch": (C.c_int32, [P, P]),
+    "enc_batch_launch_graph": (C.c_int32, [P, P]),
+    "enc_batch_check": (C.c_int32, [P, P]),
+    "enc_batch_destroy": (C.c_int32, [P]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),

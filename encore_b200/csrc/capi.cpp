@@ -651,3 +651,172 @@ enc_status enc_photonmap_nearest(enc_photonmap m, const float* qpos, const float
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Multi-scene batched launch
+
+struct enc_batch_s {
+  enc::MultiLaunch m;
+  enc::Launch L;
+  SceneDesc* d_scenes = nullptr;
+  BatchDesc* d_batches = nullptr;
+  uint32_t* d_starts = nullptr;
+  uint32_t* d_words = nullptr;  // queue head, status
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::mutex mu;
+};
+
+namespace {
+void batch_free(enc_batch b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  cudaFree(b->d_scenes);
+  cudaFree(b->d_batches);
+  cudaFree(b->d_starts);
+  cudaFree(b->d_words);
+  delete b;
+}
+}  // namespace
+
+extern "C" {
+
+enc_status enc_batch_create(const enc_batch_item* items, uint32_t nitems,
+                            const enc_launch_opts* launch, enc_batch* out) {
+  if (!out || (nitems && !items)) {
+    set_error("enc_batch_create: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  if (nitems == 0) {
+    set_error("enc_batch_create: no batches");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const DevAccel* first = accel_device_view(items[0].accel);
+  if (!first) {
+    set_error("enc_batch_create: null accelerator");
+    return ENC_ERR_INVALID_ARG;
+  }
+  Launch L = resolve_launch(launch, ENC_ACCEL_WBVH, first->width);
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 ||
+      L.chunk < 1) {
+    set_error("enc_batch_create: launch options out of range");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::vector<SceneDesc> scenes;
+  std::vector<const DevAccel*> uniq;
+  std::vector<BatchDesc> batches(nitems);
+  std::vector<uint32_t> starts(nitems + 1);
+  uint64_t pos = 0;
+  int depth = 8;
+  for (uint32_t i = 0; i < nitems; ++i) {
+    const DevAccel* a = accel_device_view(items[i].accel);
+    if (!a || (items[i].nrays && (!items[i].d_rays || !items[i].d_hits))) {
+      set_error("enc_batch_create: item " + std::to_string(i) + " has a null accelerator or buffer");
+      return ENC_ERR_INVALID_ARG;
+    }
+    if (a->kind != ENC_ACCEL_WBVH || a->width != first->width ||
+        a->predicate != first->predicate || a->device != first->device) {
+      set_error("enc_batch_create: every item needs a wide BVH of the same width, predicate and device");
+      return ENC_ERR_INVALID_ARG;
+    }
+    uint32_t si = 0;
+    while (si < uniq.size() && uniq[si] != a) ++si;
+    if (si == uniq.size()) {
+      uniq.push_back(a);
+      scenes.push_back(SceneDesc{static_cast<const uint8_t*>(a->d_nodes), a->d_tris, a->nnodes,
+                                 a->ntris});
+      depth = std::max(depth, a->tree_depth);
+    }
+    batches[i] = BatchDesc{items[i].d_rays, items[i].d_hits, si, items[i].nrays, (uint32_t)pos, 0};
+    starts[i] = (uint32_t)pos;
+    pos += ((uint64_t)items[i].nrays + L.chunk - 1) / L.chunk * L.chunk;
+    if (pos > 0x7fffffffull) {
+      set_error("enc_batch_create: more than 2^31 rays in one batch table");
+      return ENC_ERR_INVALID_ARG;
+    }
+  }
+  starts[nitems] = (uint32_t)pos;
+  DeviceScope ds(first->device);
+  enc_batch b = new (std::nothrow) enc_batch_s();
+  if (!b) return ENC_ERR_OUT_OF_MEMORY;
+  cudaError_t e = upload(&b->d_scenes, scenes.data(), scenes.size());
+  if (e == cudaSuccess) e = upload(&b->d_batches, batches.data(), batches.size());
+  if (e == cudaSuccess) e = upload(&b->d_starts, starts.data(), starts.size());
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_words, 16);
+  if (e == cudaSuccess) e = cudaMemset(b->d_words, 0, 16);
+  if (e != cudaSuccess) {
+    batch_free(b);
+    return cuda_fail(e, "enc_batch_create");
+  }
+  b->L = L;
+  MultiLaunch& m = b->m;
+  m.d_scenes = b->d_scenes;
+  m.d_batches = b->d_batches;
+  m.d_starts = b->d_starts;
+  m.nbatches = nitems;
+  m.total = (uint32_t)pos;
+  m.width = first->width;
+  m.predicate = first->predicate;
+  m.device = first->device;
+  m.stack_depth = depth;
+  m.d_counter = b->d_words;
+  m.d_status = b->d_words + 1;
+  *out = b;
+  return ENC_OK;
+}
+
+enc_status enc_batch_launch(enc_batch b, enc_stream stream) {
+  if (!b) return ENC_ERR_INVALID_ARG;
+  DeviceScope ds(b->m.device);
+  int e = launch_multi_closest(b->m, b->L, stream);
+  if (e) return cuda_fail((cudaError_t)e, "enc_batch_launch");
+  return ENC_OK;
+}
+
+enc_status enc_batch_launch_graph(enc_batch b, enc_stream stream) {
+  if (!b) return ENC_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceScope ds(b->m.device);
+  if (!b->exec) {
+    ENC_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "stream create");
+    ENC_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed), "begin capture");
+    int le = launch_multi_closest(b->m, b->L, b->cap);
+    cudaGraph_t g = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(b->cap, &g);
+    if (le) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_fail((cudaError_t)le, "enc_batch_launch_graph: capture");
+    }
+    if (ee != cudaSuccess) return cuda_fail(ee, "enc_batch_launch_graph: end capture");
+    b->graph = g;
+    ENC_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+  }
+  ENC_CUDA(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)), "graph launch");
+  return ENC_OK;
+}
+
+enc_status enc_batch_check(enc_batch b, enc_stream stream) {
+  if (!b) return ENC_ERR_INVALID_ARG;
+  DeviceScope ds(b->m.device);
+  ENC_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "cudaStreamSynchronize");
+  uint32_t st = 0;
+  ENC_CUDA(cudaMemcpy(&st, b->m.d_status, 4, cudaMemcpyDeviceToHost), "read status");
+  if (st) {
+    cudaMemset(b->m.d_status, 0, 4);
+    set_error("batched launch stopped a ray at a loop bound (status bits " + std::to_string(st) + ")");
+    return ENC_ERR_WATCHDOG;
+  }
+  return ENC_OK;
+}
+
+enc_status enc_batch_destroy(enc_batch b) {
+  if (!b) return ENC_OK;
+  DeviceScope ds(b->m.device);
+  batch_free(b);
+  return ENC_OK;
+}
+
+}  // extern "C"

@@ -97,6 +97,40 @@ struct DevAccel {
   float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
 };
 
+// ---------------------------------------------------------------------------
+// Multi-scene launch tables (device memory).  One persistent launch traces
+// the ray batches of many scenes: batch b owns queue indices
+// [start[b], start[b] + nrays), and start[b] is a multiple of the launch's
+// chunk, so a warp's chunk never spans two batches.
+struct alignas(16) SceneDesc {
+  const uint8_t* nodes;
+  const void* tris;  // DevTri[], leaf order
+  uint32_t nnodes;
+  uint32_t ntris;
+};
+struct alignas(16) BatchDesc {
+  const float* rays;  // 8 floats per ray
+  void* out;          // enc_hit[] (closest) or uint8_t[] (any)
+  uint32_t scene;
+  uint32_t nrays;
+  uint32_t start;     // first queue index of the batch
+  uint32_t any;       // 0 = closest hit, 1 = any hit (kept for the table's use by callers)
+};
+
+struct MultiLaunch {
+  const SceneDesc* d_scenes = nullptr;
+  const BatchDesc* d_batches = nullptr;
+  const uint32_t* d_starts = nullptr;  // nbatches + 1 chunk-aligned starts
+  uint32_t nbatches = 0;
+  uint32_t total = 0;  // queue indices including the alignment padding
+  int width = 8;
+  int predicate = 0;
+  int device = 0;
+  int stack_depth = 8;  // deepest scene's tree depth
+  uint32_t* d_counter = nullptr;
+  uint32_t* d_status = nullptr;
+};
+
 // Host results of the builders (before upload).
 struct WBVHHost {
   int width = 8;
@@ -138,6 +172,8 @@ int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
 int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size_t n,
                                     enc_hit* d_hits, const Launch& L, void* stream,
                                     uint32_t* counter, uint32_t* status);
+// Closest hit for every batch of a multi-scene table in one persistent launch.
+int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream);
 int device_sm_count(int device);
 
 // Error reporting (capi.cpp).

@@ -109,6 +109,11 @@ struct TraceParams {
   unsigned ntris;
   int stack_depth;
   int chunk;
+  // multi-scene launches (MULTI = true): per-batch scene and buffers
+  const SceneDesc* scenes;
+  const BatchDesc* batches;
+  const uint32_t* starts;  // nbatches + 1 chunk-aligned queue offsets
+  unsigned nbatches;
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -175,7 +180,7 @@ __device__ __forceinline__ void sort_net<8>(float (&k)[8], uint32_t (&v)[8]) {
 }
 #undef ENC_CSWAP
 
-template <int W, bool CLAMP, bool ANY, bool COUNT>
+template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false>
 __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TraceParams P) {
   using L = WNodeLayout<W>;
   // Stack of node groups: one entry per visited node that still has hit
@@ -208,6 +213,13 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
   uint32_t octm = 0;  // direction sign bits: bit a set = negative along axis a
   unsigned steps = 0;
   uint32_t nvis = 0, ntest = 0;
+  // The scene a lane's ray belongs to (MULTI: per batch, else the launch's).
+  const uint8_t* l_nodes = P.nodes;
+  const float4* l_tris = P.tris;
+  unsigned l_nnodes = P.nnodes, l_ntris = P.ntris;
+  void* l_out = P.out;
+  unsigned l_idx = 0;          // index of the ray in its output array
+  unsigned pool_batch = 0;     // MULTI: batch of the current pool
 
   while (true) {
     // ---- refill idle lanes from the warp pool --------------------------
@@ -222,14 +234,42 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
           break;
         }
         pool_next = b;
-        pool_end = min(b + (unsigned)P.chunk, P.nrays);
+        if constexpr (MULTI) {
+          // batch = last start <= b (starts are chunk-aligned, so the whole
+          // chunk lies in it); its real rays end before the padding
+          unsigned lo = 0, hi = P.nbatches;
+          while (hi - lo > 1) {
+            const unsigned mid = (lo + hi) >> 1;
+            if (__ldg(P.starts + mid) <= b) lo = mid;
+            else hi = mid;
+          }
+          pool_batch = lo;
+          pool_end = min(b + (unsigned)P.chunk, __ldg(P.starts + lo) + P.batches[lo].nrays);
+        } else {
+          pool_end = min(b + (unsigned)P.chunk, P.nrays);
+        }
       }
-      const unsigned avail = pool_end - pool_next;
+      const unsigned avail = pool_end > pool_next ? pool_end - pool_next : 0u;
       const unsigned rank = __popc(need & lt);
       if (((need >> lane) & 1u) && rank < avail) {
         ray = (int)(pool_next + rank);
-        const float4 r0 = __ldg(P.rays + 2 * (size_t)ray);
-        const float4 r1 = __ldg(P.rays + 2 * (size_t)ray + 1);
+        const float4* rp;
+        if constexpr (MULTI) {
+          const BatchDesc& bd = P.batches[pool_batch];
+          const SceneDesc& sd = P.scenes[bd.scene];
+          l_idx = (unsigned)ray - bd.start;
+          l_out = bd.out;
+          l_nodes = sd.nodes;
+          l_tris = reinterpret_cast<const float4*>(sd.tris);
+          l_nnodes = sd.nnodes;
+          l_ntris = sd.ntris;
+          rp = reinterpret_cast<const float4*>(bd.rays) + 2 * (size_t)l_idx;
+        } else {
+          l_idx = (unsigned)ray;
+          rp = P.rays + 2 * (size_t)ray;
+        }
+        const float4 r0 = __ldg(rp);
+        const float4 r1 = __ldg(rp + 1);
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
         // Box tests use a reciprocal with |d| floored at 1e-20 so that a zero
@@ -260,7 +300,7 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
         atomicOr(P.status, kStatusWatchdog);
         best_id = -1;
         done = true;
-      } else if (node >= P.nnodes) {
+      } else if (node >= l_nnodes) {
         atomicOr(P.status, kStatusBounds);
         best_id = -1;
         done = true;
@@ -270,7 +310,7 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
         //      group on the stack) ------------------------------------------
         if (COUNT) ++nvis;
         NodeWords<W> nw;
-        const uint4* src = reinterpret_cast<const uint4*>(P.nodes + (size_t)node * L::kBytes);
+        const uint4* src = reinterpret_cast<const uint4*>(l_nodes + (size_t)node * L::kBytes);
 #pragma unroll
         for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = __ldg(src + i);
         const float px = __uint_as_float(nw.w[0].x);
@@ -410,11 +450,11 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
           const uint32_t k = __ffs(trimask) - 1;
           trimask &= trimask - 1;
           const uint32_t ti = tri_base + k;
-          if (ti >= P.ntris) {
+          if (ti >= l_ntris) {
             atomicOr(P.status, kStatusBounds);
             continue;
           }
-          const float4* tp = P.tris + 3 * (size_t)ti;
+          const float4* tp = l_tris + 3 * (size_t)ti;
           const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
           if (COUNT) ++ntest;
           float t, u, v;
@@ -472,14 +512,14 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
       }
       if (done) {
         if (ANY) {
-          reinterpret_cast<uint8_t*>(P.out)[ray] = hit_any ? 1 : 0;
+          reinterpret_cast<uint8_t*>(l_out)[l_idx] = hit_any ? 1 : 0;
         } else {
           int4 h;
           h.x = best_id;
           h.y = best_id >= 0 ? __float_as_int(best_t) : 0;
           h.z = best_id >= 0 ? __float_as_int(bu) : 0;
           h.w = best_id >= 0 ? __float_as_int(bv) : 0;
-          reinterpret_cast<int4*>(P.out)[ray] = h;
+          reinterpret_cast<int4*>(l_out)[l_idx] = h;
         }
         if (COUNT) {
           P.visits[2 * (size_t)ray] = nvis;
@@ -637,7 +677,7 @@ __global__ void __launch_bounds__(128) kd_trace(KdParams P) {
 template <int W, bool CLAMP, bool ANY, bool COUNT>
 int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t* visits,
              const Launch& L, cudaStream_t s) {
-  TraceParams p;
+  TraceParams p{};
   p.nodes = static_cast<const uint8_t*>(a.d_nodes);
   p.tris = reinterpret_cast<const float4*>(a.d_tris);
   p.rays = reinterpret_cast<const float4*>(rays);
@@ -750,7 +790,7 @@ namespace {
 template <int W, bool CLAMP>
 int launch_w_external(const DevAccel& a, const float* rays, size_t n, enc_hit* hits,
                       const Launch& L, cudaStream_t s, uint32_t* counter, uint32_t* status) {
-  TraceParams p;
+  TraceParams p{};
   p.nodes = static_cast<const uint8_t*>(a.d_nodes);
   p.tris = reinterpret_cast<const float4*>(a.d_tris);
   p.rays = reinterpret_cast<const float4*>(rays);
@@ -792,6 +832,52 @@ int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size
     default:
       return clamp ? launch_w_external<8, true>(a, d_rays, n, d_hits, L, s, counter, status)
                    : launch_w_external<8, false>(a, d_rays, n, d_hits, L, s, counter, status);
+  }
+}
+
+}  // namespace enc
+
+namespace enc {
+namespace {
+
+template <int W, bool CLAMP>
+int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
+  TraceParams p{};
+  p.counter = m.d_counter;
+  p.status = m.d_status;
+  p.nrays = m.total;
+  p.stack_depth = L.stack > 0 ? L.stack : (m.stack_depth > 8 ? m.stack_depth : 8);
+  p.chunk = L.chunk;
+  p.scenes = m.d_scenes;
+  p.batches = m.d_batches;
+  p.starts = m.d_starts;
+  p.nbatches = m.nbatches;
+  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
+  auto k = wbvh_trace<W, CLAMP, false, false, true>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+  }
+  cudaError_t e = cudaMemsetAsync(m.d_counter, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return (int)e;
+  int grid = device_sm_count(m.device) * L.blocks_per_sm;
+  k<<<grid, L.block, smem, s>>>(p);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream) {
+  if (m.total == 0 || m.nbatches == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool clamp = m.predicate == ENC_PRED_REFERENCE;
+  switch (m.width) {
+    case 2:
+      return clamp ? launch_multi_w<2, true>(m, L, s) : launch_multi_w<2, false>(m, L, s);
+    case 4:
+      return clamp ? launch_multi_w<4, true>(m, L, s) : launch_multi_w<4, false>(m, L, s);
+    default:
+      return clamp ? launch_multi_w<8, true>(m, L, s) : launch_multi_w<8, false>(m, L, s);
   }
 }
 

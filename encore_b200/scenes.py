@@ -270,3 +270,52 @@ def emit_from_light(n: int, seed: int, center, size: float) -> np.ndarray:
     rays[:, 4:7] = d
     rays[:, 7] = np.inf
     return rays
+
+
+def camera_rays_jittered(n: int, seed: int, eye, look, up=(0.0, 1.0, 0.0), fov_deg: float = 45.0,
+                         res: int = 1024) -> np.ndarray:
+    """n eye rays through uniformly random points of a res x res image, the
+    jittered form of RayTracer::CalcEyeRaySamples (RayTracer.cpp:501-502)."""
+    rng = np.random.default_rng(seed)
+    eye = np.asarray(eye, dtype=F32)
+    look = np.asarray(look, dtype=F32)
+    up = np.asarray(up, dtype=F32)
+    nv = (eye - look).astype(F32)
+    u = normalize_ref(cross_ref(up, nv))
+    nv = normalize_ref(nv)
+    v = cross_ref(nv, u)
+    H = F32(np.tan(F32(fov_deg) * (float(PI_F) / 360.0)))
+    x = rng.random(n).astype(F32) * F32(res)
+    y = rng.random(n).astype(F32) * F32(res)
+    Uc = (-H + (H * (F32(2) * x) / F32(res))).astype(F32)
+    Vr = (-H + (H * (F32(2) * y) / F32(res))).astype(F32)
+    d = (-nv[None, :] + u[None, :] * Uc[:, None] + v[None, :] * Vr[:, None]).astype(F32)
+    d = normalize_ref(d)
+    rays = np.zeros((n, 8), dtype=F32)
+    rays[:, 0:3] = eye
+    rays[:, 4:7] = d
+    rays[:, 7] = np.inf
+    return rays
+
+
+def multi_scene_workload(nscenes: int = 64, seed: int = 0, scale: float = 1.0,
+                         tri_range=(1_000, 500_000), ray_range=(4_096, 1_048_576)):
+    """Scenes of random triangles with log-uniform triangle counts, each with a
+    log-uniform-sized ray batch, half camera rays and half uniform-sphere rays.
+    Returns (list of (N_i, 9) triangle arrays, list of (M_i, 8) ray arrays)."""
+    rng = np.random.default_rng(seed)
+    lt = np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]), nscenes)).astype(int)
+    lr = np.exp(rng.uniform(np.log(ray_range[0]), np.log(ray_range[1]), nscenes)).astype(int)
+    tris, rays = [], []
+    for i in range(nscenes):
+        t = random_triangles(int(lt[i]), seed=seed * 1000 + 2 * i, scale=scale)
+        m = int(lr[i])
+        cam = camera_rays_jittered(m // 2, seed=seed * 1000 + 2 * i + 1,
+                                   eye=np.array([0.5, 0.5, -1.5]) * scale,
+                                   look=np.array([0.5, 0.5, 0.5]) * scale)
+        sph = random_sphere_rays(m - m // 2, seed=seed * 1000 + 2 * i + 2,
+                                 hi=(scale, scale, scale))
+        r = np.concatenate([cam, sph])
+        rays.append(np.ascontiguousarray(r[rng.permutation(m)]))
+        tris.append(t)
+    return tris, rays

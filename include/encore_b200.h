@@ -176,6 +176,30 @@ enc_status enc_accel_count_visits(enc_accel accel, const float* d_rays, size_t n
 enc_status enc_intersect_closest_noalloc(enc_accel accel, const float* rays, size_t nrays,
                                          enc_hit* hits, enc_stream stream);
 
+/* ---- Multi-scene batched launch ------------------------------------------
+ * No counterpart in the reference (it traces one ray per call).  Ray batches
+ * of many scenes are traced by one persistent launch: warps take chunks of
+ * rays from one queue that spans every batch, so small batches share the GPU
+ * with large ones instead of each paying a launch and a tail.  The launch can
+ * be recorded once into a CUDA graph and replayed. */
+typedef struct enc_batch_s* enc_batch;
+typedef struct enc_batch_item {
+  enc_accel accel;     /* wide BVH; all items: same device, width, predicate */
+  const float* d_rays; /* device memory, 8 floats per ray */
+  enc_hit* d_hits;     /* device memory, one enc_hit per ray */
+  uint32_t nrays;
+  uint32_t reserved;   /* 0 */
+} enc_batch_item;
+enc_status enc_batch_create(const enc_batch_item* items, uint32_t nitems,
+                            const enc_launch_opts* launch, enc_batch* out);
+/* One launch over every batch; asynchronous on `stream`. */
+enc_status enc_batch_launch(enc_batch batch, enc_stream stream);
+/* The same launch, captured into a CUDA graph on first use and replayed. */
+enc_status enc_batch_launch_graph(enc_batch batch, enc_stream stream);
+/* Waits for `stream`; ENC_ERR_WATCHDOG if a ray stopped at a loop bound. */
+enc_status enc_batch_check(enc_batch batch, enc_stream stream);
+enc_status enc_batch_destroy(enc_batch batch);
+
 /* PhotonMap: AddPhoton x n followed by BalanceAndConstruct
  * (PhotonMap.cpp:46-53, 167-221).  caustic != 0 selects the caustic-map
  * estimate (cone weight and N/(pi r^2), PhotonMap.cpp:147, 157). */
