@@ -238,6 +238,211 @@ def read_profile_traffic() -> float | None:
     return None
 
 
+def batched_section(dev: int, args, flush) -> dict:
+    """64 scenes of random triangles (log-uniform 1k-500k), one ray batch
+    each (log-uniform 4k-1M, half camera, half uniform-sphere rays): every
+    batch launched on its own back to back (plain) vs one persistent launch
+    over all batches replayed from a CUDA graph (batched), with the launch
+    shape and BVH width from the autotuner."""
+    import torch
+    from encore_b200 import Accelerator, scenes
+    from encore_b200.autotune import autotune, launch_config
+    from encore_b200.batch import BatchLaunch
+    t0 = time.perf_counter()
+    tris, rays = scenes.multi_scene_workload(64, seed=33, scale=SCALE)
+    total = sum(len(r) for r in rays)
+    tune_idx = list(range(0, 64, 4))
+    rep = autotune([tris[i] for i in tune_idx], [rays[i] for i in tune_idx], widths=(4, 8),
+                   chunks=(16, 32, 64), blocks_per_sm=(8,), block_threads=(128,), reps=3,
+                   device=dev)
+    width, lc = launch_config(rep["best"])
+    accs8 = [Accelerator("wbvh", width=8, device=dev).build(t) for t in tris]
+    accs = accs8 if width == 8 else [Accelerator("wbvh", width=width, device=dev).build(t)
+                                     for t in tris]
+    stream = torch.cuda.current_stream()
+    d_rays = [torch.from_numpy(r).to(dev) for r in rays]
+    d_plain = [torch.empty((len(r), 4), dtype=torch.int32, device=dev) for r in rays]
+    d_bat = [torch.empty((len(r), 4), dtype=torch.int32, device=dev) for r in rays]
+    b = BatchLaunch(list(zip(accs, d_rays, d_bat)), launch=lc)
+    log(f"batched section inputs in {time.perf_counter() - t0:.1f}s: {total} rays, "
+        f"{sum(len(t) for t in tris)} tris; tuned width {width} chunk {lc.chunk}")
+
+    def plain():
+        for a, r, h in zip(accs8, d_rays, d_plain):
+            a.intersect_device(r, r.shape[0], h, stream=stream)
+
+    def batched():
+        b.launch_graph(stream=stream)
+
+    out = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out[name] = total * len(ts) / (sum(ts) * 1e-3) / 1e6
+    b.check(stream)
+    for a in accs8:
+        a.check(stream)
+    same = all(torch.equal(p[:, 0], q[:, 0]) for p, q in zip(d_plain, d_bat))
+    b.destroy()
+    for a in set(accs8) | set(accs):
+        a.destroy()
+    return {"workload": "64 random-triangle scenes (1k-500k tris), 4k-1M rays each, x1000",
+            "rays": total, "plain_mrays_s": round(out["plain"], 1),
+            "batched_mrays_s": round(out["batched"], 1),
+            "batched_over_plain": round(out["batched"] / out["plain"], 3),
+            "same_hits": bool(same), "tuned": rep["best"], "launches_plain": 64,
+            "launches_batched": 1}
+
+
+def served_section(dev: int, args) -> dict:
+    """32 resident scenes (16 random-triangle scenes of 1k-2M triangles, 16
+    1024x1024 heightfields with different seeds), requests of log-uniform
+    16k-4M rays on a uniform-random scene, 60 % camera / 30 % diffuse
+    closest-hit and 10 % shadow any-hit.  Saturation throughput of the server
+    (all requests submitted at once) vs the plain per-request call run back to
+    back; latency under Poisson arrivals at 60 % of the served throughput."""
+    import torch
+    from encore_b200 import Accelerator, scenes
+    from encore_b200.serving import ANY, CLOSEST, Server
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(44)
+    tris = [scenes.random_triangles(int(np.exp(rng.uniform(np.log(1e3), np.log(2e6)))),
+                                    seed=4400 + i, scale=SCALE) for i in range(16)]
+    tris += [scenes.heightfield(res=RES, seed=4500 + i, scale=SCALE) for i in range(16)]
+    accs = [Accelerator("wbvh", device=dev).build(t) for t in tris]
+    npool = 24
+    pool = []
+    for j in range(npool):
+        s = int(rng.integers(0, 32))
+        n = int(np.exp(rng.uniform(np.log(16384), np.log(4 << 20))))
+        u = rng.random()
+        if u < 0.6:
+            if s >= 16:  # heightfield: the top-down camera of the main workload
+                cam = dict(eye=np.array([0.5, 1.3, 0.5]) * SCALE,
+                           look=np.array([0.5, 0.0, 0.5]) * SCALE, up=(0.0, 0.0, 1.0),
+                           fov_deg=40.0)
+            else:
+                cam = dict(eye=np.array([0.5, 0.5, -1.5]) * SCALE,
+                           look=np.array([0.5, 0.5, 0.5]) * SCALE)
+            r, k = scenes.camera_rays_jittered(n, 4600 + j, **cam), CLOSEST
+        elif u < 0.9:
+            r, k = scenes.surface_rays(tris[s], n, 4600 + j, "diffuse", offset=0.1,
+                                       up_facing=s >= 16), CLOSEST
+        else:
+            r, k = scenes.surface_rays(tris[s], n, 4600 + j, "shadow", light_center=LIGHT,
+                                       light_size=0.1 * SCALE, offset=0.01 * SCALE), ANY
+        hr = torch.from_numpy(np.ascontiguousarray(r)).pin_memory()
+        ho = torch.empty((n, 4) if k == CLOSEST else (n,), dtype=torch.int32 if k == CLOSEST
+                         else torch.uint8).pin_memory()
+        pool.append((s, k, n, hr, ho))
+    total = sum(p[2] for p in pool)
+    log(f"served section inputs in {time.perf_counter() - t0:.1f}s: {total} rays in {npool} requests")
+
+    def out_view(p):
+        from encore_b200.accel import HIT_DTYPE
+        return p[4].numpy().view(HIT_DTYPE).reshape(p[2]) if p[1] == CLOSEST else p[4].numpy()
+
+    # plain: the per-request host-buffer call, back to back
+    svc = []
+    for rep in range(2):
+        svc = []
+        for p in pool:
+            t1 = time.perf_counter()
+            if p[1] == CLOSEST:
+                accs[p[0]].intersect(p[3].numpy(), out=out_view(p))
+            else:
+                accs[p[0]].occluded(p[3].numpy(), out=out_view(p))
+            svc.append(time.perf_counter() - t1)
+    plain_rate = total / sum(svc) / 1e6
+    plain_ref = [out_view(p).copy() for p in pool]
+
+    srv = Server(device=dev, slots=3, slot_rays=8 << 20)
+    ids = [srv.add_scene(a) for a in accs]
+    sat = []
+    for rep in range(2):
+        t1 = time.perf_counter()
+        rids = [srv.submit(ids[p[0]], p[3].numpy(), p[1], out=out_view(p)) for p in pool]
+        for rid in rids:
+            srv.wait(rid)
+        sat.append(time.perf_counter() - t1)
+    served_rate = total / min(sat) / 1e6
+    same = all(np.array_equal(out_view(p).view(np.uint8), ref.view(np.uint8))
+               for p, ref in zip(pool, plain_ref))
+
+    # latency under Poisson arrivals (ring of pooled requests, 3 passes)
+    nreq = 3 * npool
+    mean_rays = total / npool
+    lam = 0.6 * served_rate * 1e6 / mean_rays  # requests per second
+    gaps = rng.exponential(1.0 / lam, nreq)
+    arrivals = np.cumsum(gaps)
+    lat, sizes = [], []
+    start = srv.now() + 0.01
+    rids = [None] * nreq
+    done = threading.Event()
+
+    def submitter():
+        for j in range(nreq):
+            if j >= npool:  # reuse pooled buffers only after their last request finished
+                while not waited[j - npool]:
+                    time.sleep(0.0001)
+            dt = start + arrivals[j] - srv.now()
+            if dt > 0.001:
+                time.sleep(dt - 0.0005)
+            while srv.now() < start + arrivals[j]:
+                pass
+            p = pool[j % npool]
+            rids[j] = srv.submit(ids[p[0]], p[3].numpy(), p[1], out=out_view(p))
+        done.set()
+
+    waited = [False] * nreq
+    th = threading.Thread(target=submitter)
+    th.start()
+    for j in range(nreq):
+        while rids[j] is None:
+            time.sleep(0.00005)
+        _, info = srv.wait(rids[j])
+        lat.append(info["done_s"] - info["submit_s"])
+        sizes.append(info["nrays"])
+        waited[j] = True
+    th.join()
+    srv.destroy()
+    # the plain per-request server under the same arrivals (FIFO, one call at a time)
+    plain_lat, finish = [], 0.0
+    for j in range(nreq):
+        a = arrivals[j]
+        finish = max(finish, a) + svc[j % npool]
+        plain_lat.append(finish - a)
+    lat = np.array(lat) * 1e3
+    plain_lat = np.array(plain_lat) * 1e3
+    sizes = np.array(sizes)
+    m1 = (sizes >= (512 << 10)) & (sizes <= (2 << 20))
+    for a in accs:
+        a.destroy()
+    return {"workload": "32 resident scenes (16 random 1k-2M tris, 16 heightfields 2.1M tris), "
+                        "requests 16k-4M rays, 60/30/10 camera/diffuse/shadow, x1000",
+            "requests": npool, "rays": int(total),
+            "plain_mrays_s": round(plain_rate, 1), "served_mrays_s": round(served_rate, 1),
+            "served_over_plain": round(served_rate / plain_rate, 3), "same_hits": bool(same),
+            "poisson_offered_load": 0.6, "poisson_requests": nreq,
+            "p50_ms": round(float(np.percentile(lat, 50)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "p99_ms_1M_requests": (round(float(np.percentile(lat[m1], 99)), 3) if m1.any() else None),
+            "plain_p50_ms": round(float(np.percentile(plain_lat, 50)), 3),
+            "plain_p99_ms": round(float(np.percentile(plain_lat, 99)), 3),
+            "copies": "host pinned buffers, copies inside every request"}
+
+
 def run_engine_arm(args, rank: int, world: int) -> None:
     import torch
     import torch.distributed as dist
@@ -376,6 +581,15 @@ def run_engine_arm(args, rank: int, world: int) -> None:
                          f"Kdtree::intersect on {cores} host threads; Kdtree build "
                          f"{build_s:.1f} s not timed"}
 
+    acc.destroy()
+    del d_rays, d_hits, d_shadow, d_occ, h_rays, h_hits
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        torch.cuda.empty_cache()
+        extras["batched"] = batched_section(dev, args, flush)
+        torch.cuda.empty_cache()
+        extras["served"] = served_section(dev, args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
@@ -401,9 +615,9 @@ def run_engine_arm(args, rank: int, world: int) -> None:
             "build_seconds": round(info["build_seconds"], 3),
             "clocks": clk,
             "cpu_baseline": cpu,
+            **extras,
         }
         print(json.dumps(line), flush=True)
-    acc.destroy()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -422,6 +636,8 @@ def main():
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--stack", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched multi-scene and served sections")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up below 3 steps is not a valid measurement; using 3")

@@ -64,6 +64,16 @@ class BatchItem(C.Structure):
                 ("nrays", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("slot_rays", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("launch", LaunchOpts)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("submit_s", C.c_double), ("start_s", C.c_double), ("done_s", C.c_double),
+                ("nrays", C.c_uint64), ("status", C.c_int32), ("kind", C.c_int32)]
+
+
 P = C.c_void_p
 F = C.POINTER(C.c_float)
 
@@ -90,6 +100,14 @@ SIGNATURES = {
     "enc_batch_launch_graph": (C.c_int32, [P, P]),
     "enc_batch_check": (C.c_int32, [P, P]),
     "enc_batch_destroy": (C.c_int32, [P]),
+    "enc_server_create": (C.c_int32, [C.POINTER(ServerOpts), C.POINTER(P)]),
+    "enc_server_add_scene": (C.c_int32, [P, P, C.POINTER(C.c_uint32)]),
+    "enc_server_submit": (C.c_int32, [P, C.c_uint32, C.c_int32, P, C.c_uint64, P,
+                                      C.POINTER(C.c_uint64)]),
+    "enc_server_wait": (C.c_int32, [P, C.c_uint64, C.c_double, C.POINTER(RequestInfo)]),
+    "enc_server_cancel": (C.c_int32, [P, C.c_uint64]),
+    "enc_server_now": (C.c_double, []),
+    "enc_server_destroy": (C.c_int32, [P]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),

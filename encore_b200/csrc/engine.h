@@ -174,6 +174,8 @@ int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size
                                     uint32_t* counter, uint32_t* status);
 // Closest hit for every batch of a multi-scene table in one persistent launch.
 int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream);
+// Any hit (uint8 occluded per ray) for every batch of the table.
+int launch_multi_any(const MultiLaunch& m, const Launch& L, void* stream);
 int device_sm_count(int device);
 
 // Error reporting (capi.cpp).

@@ -840,7 +840,7 @@ int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size
 namespace enc {
 namespace {
 
-template <int W, bool CLAMP>
+template <int W, bool CLAMP, bool ANY>
 int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   TraceParams p{};
   p.counter = m.d_counter;
@@ -853,7 +853,7 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   p.starts = m.d_starts;
   p.nbatches = m.nbatches;
   size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
-  auto k = wbvh_trace<W, CLAMP, false, false, true>;
+  auto k = wbvh_trace<W, CLAMP, ANY, false, true>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
@@ -865,20 +865,29 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   return (int)cudaGetLastError();
 }
 
-}  // namespace
-
-int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream) {
+template <bool ANY>
+int launch_multi(const MultiLaunch& m, const Launch& L, void* stream) {
   if (m.total == 0 || m.nbatches == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool clamp = m.predicate == ENC_PRED_REFERENCE;
   switch (m.width) {
     case 2:
-      return clamp ? launch_multi_w<2, true>(m, L, s) : launch_multi_w<2, false>(m, L, s);
+      return clamp ? launch_multi_w<2, true, ANY>(m, L, s) : launch_multi_w<2, false, ANY>(m, L, s);
     case 4:
-      return clamp ? launch_multi_w<4, true>(m, L, s) : launch_multi_w<4, false>(m, L, s);
+      return clamp ? launch_multi_w<4, true, ANY>(m, L, s) : launch_multi_w<4, false, ANY>(m, L, s);
     default:
-      return clamp ? launch_multi_w<8, true>(m, L, s) : launch_multi_w<8, false>(m, L, s);
+      return clamp ? launch_multi_w<8, true, ANY>(m, L, s) : launch_multi_w<8, false, ANY>(m, L, s);
   }
+}
+
+}  // namespace
+
+int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream) {
+  return launch_multi<false>(m, L, stream);
+}
+
+int launch_multi_any(const MultiLaunch& m, const Launch& L, void* stream) {
+  return launch_multi<true>(m, L, stream);
 }
 
 }  // namespace enc

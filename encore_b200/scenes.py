@@ -319,3 +319,32 @@ def multi_scene_workload(nscenes: int = 64, seed: int = 0, scale: float = 1.0,
         rays.append(np.ascontiguousarray(r[rng.permutation(m)]))
         tris.append(t)
     return tris, rays
+
+
+def surface_rays(tris: np.ndarray, n: int, seed: int, kind: str = "diffuse", light_center=None,
+                 light_size: float = 0.1, offset: float = 1e-4, up_facing: bool = False) -> np.ndarray:
+    """Rays leaving random points on random triangles of a scene: `diffuse`
+    (cosine-weighted about the triangle normal, on a random side, or the +y
+    side with up_facing) or `shadow` (toward a random point of a square light
+    facing -y, tmax = distance, origin pushed `offset` along the ray)."""
+    rng = np.random.default_rng(seed)
+    t = tris.reshape(-1, 3, 3).astype(np.float64)
+    ids = rng.integers(0, len(t), size=n)
+    r1 = np.sqrt(rng.random(n))
+    r2 = rng.random(n)
+    p = ((1 - r1)[:, None] * t[ids, 0] + (r1 * (1 - r2))[:, None] * t[ids, 1]
+         + (r1 * r2)[:, None] * t[ids, 2])
+    if kind == "shadow":
+        return shadow_rays(p.astype(F32), seed + 1, light_center, light_size, offset)
+    nrm = np.cross(t[ids, 1] - t[ids, 0], t[ids, 2] - t[ids, 0])
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-300)
+    if up_facing:
+        nrm *= np.where(nrm[:, 1:2] < 0, -1.0, 1.0)
+    else:
+        nrm *= np.where(rng.random((n, 1)) < 0.5, -1.0, 1.0)
+    d = cosine_directions(nrm, rng)
+    rays = np.zeros((n, 8), dtype=F32)
+    rays[:, 0:3] = p + offset * nrm
+    rays[:, 4:7] = d
+    rays[:, 7] = np.inf
+    return rays

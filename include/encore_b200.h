@@ -200,6 +200,55 @@ enc_status enc_batch_launch_graph(enc_batch batch, enc_stream stream);
 enc_status enc_batch_check(enc_batch batch, enc_stream stream);
 enc_status enc_batch_destroy(enc_batch batch);
 
+/* ---- Serving ---------------------------------------------------------------
+ * No counterpart in the reference.  A server keeps a pool of accelerators
+ * resident in HBM and answers ray-batch requests with continuous batching: a
+ * scheduler thread admits queued requests, in arrival order, into launch
+ * slots as slots and slot memory free up; every admitted group is traced by
+ * one fused multi-scene launch (plus one for any-hit requests) whose copies
+ * run on the slot's own stream, so requests that arrive while others are on
+ * the GPU overlap with them.  Resident scenes and slot buffers are counted
+ * against an HBM budget. */
+typedef struct enc_server_s* enc_server;
+typedef struct enc_server_opts {
+  int32_t device;
+  uint32_t slots;          /* launches in flight at once (0 = 3) */
+  uint64_t slot_rays;      /* ray capacity of one slot; a request may not exceed it
+                              (0 = 8,388,608) */
+  uint64_t budget_bytes;   /* HBM budget: resident scenes + slot buffers (0 = 120 GB) */
+  enc_launch_opts launch;  /* kernel launch shape (zeros = defaults) */
+} enc_server_opts;
+enum { ENC_REQ_CLOSEST = 0, ENC_REQ_ANY = 1 };
+typedef struct enc_request_info {
+  double submit_s;   /* steady-clock seconds at submit */
+  double start_s;    /* when its slot's copies were enqueued */
+  double done_s;     /* when its results were in host memory */
+  uint64_t nrays;
+  int32_t status;    /* enc_status of the request */
+  int32_t kind;
+} enc_request_info;
+
+enc_status enc_server_create(const enc_server_opts* opts, enc_server* out);
+/* Adds a resident scene (a wide BVH built on the server's device); the
+ * server does not take ownership.  ENC_ERR_BUDGET if it does not fit. */
+enc_status enc_server_add_scene(enc_server server, enc_accel accel, uint32_t* scene_id);
+/* Queues a request.  rays: host memory, 8 floats per ray (pinned memory lets
+ * the copies overlap); out: host memory, enc_hit per ray (closest) or one
+ * byte per ray (any); both must stay valid until the request completes. */
+enc_status enc_server_submit(enc_server server, uint32_t scene_id, int32_t kind,
+                             const float* rays, uint64_t nrays, void* out, uint64_t* request_id);
+/* Waits up to timeout_s (< 0: forever) for a request; ENC_ERR_NOT_READY on
+ * timeout.  info may be NULL.  A finished request is forgotten after it has
+ * been waited for. */
+enc_status enc_server_wait(enc_server server, uint64_t request_id, double timeout_s,
+                           enc_request_info* info);
+/* Cancels a request that has not been admitted yet (ENC_ERR_NOT_READY if it
+ * already runs). */
+enc_status enc_server_cancel(enc_server server, uint64_t request_id);
+/* Steady-clock seconds (the clock of enc_request_info). */
+double enc_server_now(void);
+enc_status enc_server_destroy(enc_server server);
+
 /* PhotonMap: AddPhoton x n followed by BalanceAndConstruct
  * (PhotonMap.cpp:46-53, 167-221).  caustic != 0 selects the caustic-map
  * estimate (cone weight and N/(pi r^2), PhotonMap.cpp:147, 157). */
