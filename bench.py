@@ -443,6 +443,97 @@ def served_section(dev: int, args) -> dict:
             "copies": "host pinned buffers, copies inside every request"}
 
 
+def gather_section(dev: int, args, flush) -> dict:
+    """Photon mapping on the 10,000-random-triangle scene: 2M photons emitted
+    from a 0.1 x 0.1 light at height 2.0 (cosine lobe, power 1/N, up to 3
+    diffuse bounces, Russian roulette at albedo 0.7) traced on the GPU, one
+    photon map, then a k = 50, r = 0.02 radiance gather at 1M primary-hit
+    points (x1000 scale: r = 20)."""
+    import torch
+    from encore_b200 import Accelerator, scenes, wavefront
+    from oracle import bindings as ob
+    t0 = time.perf_counter()
+    tris = scenes.random_triangles(10000, seed=0, scale=SCALE)
+    acc = Accelerator("wbvh", device=dev).build(tris)
+    nph, cap = 2_000_000, 8_000_000
+    bufs = [torch.empty((cap, 3), dtype=torch.float32, device=dev) for _ in range(3)]
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    m = wavefront.trace_photons(acc, LIGHT, 0.1 * SCALE, nph, *bufs, max_bounces=3, albedo=0.7,
+                                seed=7, emit_offset=0.01 * SCALE, bounce_offset=0.001 * SCALE)
+    trace_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    pm = wavefront.photon_map_from_device(bufs[0], bufs[1], bufs[2], m, device=dev)
+    build_s = time.perf_counter() - t1
+    side = 1536
+    d_rays = torch.empty((side * side, 8), dtype=torch.float32, device=dev)
+    wavefront.camera_rays(np.array([0.5, 0.5, -1.5]) * SCALE, np.array([0.5, 0.5, 0.5]) * SCALE,
+                          (0.0, 1.0, 0.0), 45.0, side, side, d_rays)
+    d_hits = torch.empty((side * side, 4), dtype=torch.int32, device=dev)
+    acc.intersect_device(d_rays, side * side, d_hits)
+    d_p = torch.empty((side * side, 3), dtype=torch.float32, device=dev)
+    d_n = torch.empty((side * side, 3), dtype=torch.float32, device=dev)
+    wavefront.hit_surface(acc, d_hits, side * side, d_p, d_n)
+    ok = d_hits[:, 0] >= 0
+    q = d_p[ok][: 1 << 20].contiguous()
+    qn = d_n[ok][: 1 << 20].contiguous()
+    nq = q.shape[0]
+    d_rgb = torch.empty((nq, 3), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    k, r = 50, 0.02 * SCALE
+    for _ in range(3):
+        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    rate = nq * len(ts) / (sum(ts) * 1e-3) / 1e6
+    # parity sample against the FP64 oracle on the same photons
+    pos, nrm, pw = (b[:m].cpu().numpy() for b in bufs)
+    sel = np.linspace(0, nq - 1, 2000).astype(int)
+    qs, qns = q.cpu().numpy()[sel], qn.cpu().numpy()[sel]
+    want, cnt = ob.port_gather(pos, nrm, pw, qs, qns, k, r)
+    got = d_rgb.cpu().numpy()[sel]
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
+    cpu = None
+    if not args.no_cpu and ob.reference() is not None:
+        import ctypes as C
+        lib = ob.reference()
+        bs = C.c_double()
+        h = lib.encref_pmap_create(pos.ctypes.data, nrm.ctypes.data, pw.ctypes.data, m, 0,
+                                   C.byref(bs))
+        out = np.empty((len(qs), 3), np.float32)
+        nt = os.cpu_count() or 1
+        t1 = time.perf_counter()
+        lib.encref_pmap_radiance(h, np.ascontiguousarray(qs).ctypes.data,
+                                 np.ascontiguousarray(qns).ctypes.data, len(qs), k, r,
+                                 out.ctypes.data, nt)
+        cpu_s = time.perf_counter() - t1
+        lib.encref_pmap_destroy(h)
+        cpu = {"value": round(len(qs) / cpu_s / 1e6, 6), "unit": "Mqueries/s", "cores": nt,
+               "kind": "reference", "build_seconds": round(bs.value, 2),
+               "sample": f"{len(qs)} of the same queries, PhotonMap::GetRadianceEstimate"}
+        ref_rel = np.abs(got - out) / np.maximum(np.abs(out), 1e-30)
+        cpu["max_rel_err_vs_reference"] = float(ref_rel.max())
+    pm._destroy()
+    acc.destroy()
+    log(f"gather section in {time.perf_counter() - t0:.1f}s: {m} photons stored, {nq} queries")
+    return {"workload": "10k random triangles x1000, 2M photons (<=3 bounces, RR 0.7), "
+                        "k=50 r=0.02 (x1000) at primary hits",
+            "photons_emitted": nph, "photons_stored": int(m),
+            "photon_trace_ms": round(trace_s * 1e3, 2), "photon_map_build_s": round(build_s, 3),
+            "queries": int(nq), "mqueries_s": round(rate, 2),
+            "ms_per_gather": round(sum(ts) / len(ts), 3),
+            "found_mean": float(cnt.mean()),
+            "max_rel_err_vs_fp64": float(rel.max()), "cpu_baseline": cpu}
+
+
 def run_engine_arm(args, rank: int, world: int) -> None:
     import torch
     import torch.distributed as dist
@@ -589,6 +680,8 @@ def run_engine_arm(args, rank: int, world: int) -> None:
         extras["batched"] = batched_section(dev, args, flush)
         torch.cuda.empty_cache()
         extras["served"] = served_section(dev, args)
+        torch.cuda.empty_cache()
+        extras["photon_gather"] = gather_section(dev, args, flush)
 
     if rank == 0:
         line = {

@@ -74,6 +74,18 @@ class RequestInfo(C.Structure):
                 ("nrays", C.c_uint64), ("status", C.c_int32), ("kind", C.c_int32)]
 
 
+class Camera(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("look", C.c_float * 3), ("up", C.c_float * 3),
+                ("fov_deg", C.c_float), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("jitter_seed", C.c_uint32)]
+
+
+class PhotonOpts(C.Structure):
+    _fields_ = [("light_center", C.c_float * 3), ("light_size", C.c_float),
+                ("nphotons", C.c_uint32), ("max_bounces", C.c_uint32), ("albedo", C.c_float),
+                ("seed", C.c_uint32), ("emit_offset", C.c_float), ("bounce_offset", C.c_float)]
+
+
 P = C.c_void_p
 F = C.POINTER(C.c_float)
 
@@ -108,6 +120,14 @@ SIGNATURES = {
     "enc_server_cancel": (C.c_int32, [P, C.c_uint64]),
     "enc_server_now": (C.c_double, []),
     "enc_server_destroy": (C.c_int32, [P]),
+    "enc_camera_rays_device": (C.c_int32, [C.POINTER(Camera), P, P]),
+    "enc_hit_surface_device": (C.c_int32, [P, P, C.c_size_t, P, P, P]),
+    "enc_diffuse_rays_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_uint32, C.c_uint32,
+                                            C.c_float, P, P]),
+    "enc_photons_trace_device": (C.c_int32, [P, C.POINTER(PhotonOpts), P, P, P, C.c_uint32,
+                                             C.POINTER(C.c_uint32), P]),
+    "enc_photonmap_create_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32,
+                                                C.POINTER(P)]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),

@@ -86,6 +86,8 @@ void free_dev(DevAccel& a) {
   cudaFree(a.d_tris);
   cudaFree(a.d_kd);
   cudaFree(a.d_kd_items);
+  cudaFree(a.d_tri_pos);
+  a.d_tri_pos = nullptr;
   cudaFree(a.d_status);
   cudaFree(a.d_counter);
   a.d_nodes = nullptr;
@@ -252,6 +254,7 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
       e = upload(&dn, h.nodes.data(), h.nodes.size());
       d.d_nodes = dn;
       if (e == cudaSuccess) e = upload(&d.d_tris, h.tris.data(), h.tris.size());
+      if (e == cudaSuccess) e = upload(&d.d_tri_pos, h.tri_pos.data(), h.tri_pos.size());
       d.node_bytes = h.nodes.size();
       d.tri_bytes = h.tris.size() * sizeof(DevTri);
     } else {
@@ -293,7 +296,8 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
     delete a;
     return cuda_fail(e, "enc_accel_build: upload");
   }
-  d.device_bytes = d.node_bytes + d.tri_bytes + 32;
+  d.device_bytes = d.node_bytes + d.tri_bytes + (d.d_tri_pos ? 4ull * d.ntris : 0) +
+                   kQueueSlots * sizeof(uint32_t) + 16;
   d.build_seconds = now_s() - t0;
   *out = a;
   return ENC_OK;
@@ -540,6 +544,25 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
   }
   *out = m;
   return ENC_OK;
+}
+
+enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, const float* d_pow,
+                                       size_t n, int32_t caustic, int32_t device,
+                                       enc_photonmap* out) {
+  if (!out || (n && (!d_pos || !d_nrm || !d_pow))) {
+    set_error("enc_photonmap_create_device: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::vector<float> pos(3 * n), nrm(3 * n), pw(3 * n);
+  {
+    DeviceScope ds(device);
+    if (n) {
+      ENC_CUDA(cudaMemcpy(pos.data(), d_pos, 12 * n, cudaMemcpyDeviceToHost), "D2H photons");
+      ENC_CUDA(cudaMemcpy(nrm.data(), d_nrm, 12 * n, cudaMemcpyDeviceToHost), "D2H photons");
+      ENC_CUDA(cudaMemcpy(pw.data(), d_pow, 12 * n, cudaMemcpyDeviceToHost), "D2H photons");
+    }
+  }
+  return enc_photonmap_create(pos.data(), nrm.data(), pw.data(), n, caustic, device, out);
 }
 
 enc_status enc_photonmap_destroy(enc_photonmap m) {

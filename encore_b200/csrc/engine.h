@@ -79,6 +79,7 @@ struct DevAccel {
   // WBVH
   void* d_nodes = nullptr;      // nnodes * WNodeLayout<W>::kBytes
   DevTri* d_tris = nullptr;     // WBVH: leaf order; kd: triangle-ID order
+  uint32_t* d_tri_pos = nullptr;  // triangle ID -> index into d_tris (WBVH; kd: identity, null)
   // kd-tree
   KdNode* d_kd = nullptr;
   uint32_t* d_kd_items = nullptr;  // leaf triangle IDs
@@ -137,6 +138,7 @@ struct WBVHHost {
   std::vector<uint8_t> nodes;  // nnodes * kBytes
   uint32_t nnodes = 0;
   std::vector<DevTri> tris;    // leaf order
+  std::vector<uint32_t> tri_pos;  // triangle ID -> position in `tris`
   float lo[3], hi[3];
   int depth = 0;               // levels of wide nodes (root = 1)
 };

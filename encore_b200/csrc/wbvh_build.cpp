@@ -332,6 +332,8 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
   }
   out->nnodes = (uint32_t)queue.size();
   out->depth = max_level;
+  out->tri_pos.assign(tri_order.size(), 0);
+  for (size_t i = 0; i < tri_order.size(); ++i) out->tri_pos[tri_order[i]] = (uint32_t)i;
   out->tris.resize(tri_order.size());
   make_dev_tris(tri_verts, (uint32_t)tri_order.size(), tri_order.data(), out->tris.data());
 }

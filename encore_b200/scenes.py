@@ -143,7 +143,9 @@ def camera_rays(width: int, height: int, eye, look, up=(0.0, 1.0, 0.0), fov_deg:
     n = normalize_ref(n)
     u = normalize_ref(u)
     v = cross_ref(n, u)
-    H = F32(near * np.tan(F32(fov_deg) * (float(PI_F) / 360.0)))
+    # H = near * tan(angle * (PI / 360.0)) evaluated in double, as the float
+    # angle times the double constant promotes (RayTracer.cpp:495)
+    H = F32(near * np.tan(np.float64(F32(fov_deg)) * (float(PI_F) / 360.0)))
     W = F32(H * F32(width / height))
     cols = np.arange(width, dtype=F32) + F32(0.5)
     rows = np.arange(height, dtype=F32) + F32(0.5)

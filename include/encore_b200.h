@@ -249,6 +249,56 @@ enc_status enc_server_cancel(enc_server server, uint64_t request_id);
 double enc_server_now(void);
 enc_status enc_server_destroy(enc_server server);
 
+/* ---- Ray and photon generation on the device ------------------------------ */
+typedef struct enc_camera {
+  float eye[3], look[3], up[3];
+  float fov_deg;         /* vertical field of view */
+  uint32_t width, height;
+  uint32_t jitter_seed;  /* 0: pixel centres; otherwise a seeded random point per pixel */
+} enc_camera;
+/* One eye ray per pixel, row-major from the bottom row, formed as
+ * RayTracer::CalcEyeRaySamples does (RayTracer.cpp:489-525) with the basis of
+ * Camera::CalcCamVectors (Camera.cpp:157-166): FP32, clamping Cross and
+ * Normalize, near plane 1.  d_rays: width*height rays. */
+enc_status enc_camera_rays_device(const enc_camera* cam, float* d_rays, enc_stream stream);
+/* Hit point v0 + (v1-v0)*alpha + (v2-v0)*beta and the normal
+ * Normalize(Cross(edge1, edge2)) that TrianglePrim::intersect stores
+ * (TrianglePrim.cpp:236-239), 3 floats each per hit; NaN for misses. */
+enc_status enc_hit_surface_device(enc_accel accel, const enc_hit* d_hits, size_t n, float* d_pos,
+                                  float* d_nrm, enc_stream stream);
+/* per_hit cosine-weighted diffuse rays from each closest hit, origin pushed
+ * `offset` along the normal facing the incoming ray; output ray i*per_hit+k
+ * belongs to hit i, misses give empty rays (tmax = 0).  Seeded, independent of
+ * the launch shape. */
+enc_status enc_diffuse_rays_device(enc_accel accel, const float* d_rays, const enc_hit* d_hits,
+                                   size_t n, uint32_t per_hit, uint32_t seed, float offset,
+                                   float* d_out, enc_stream stream);
+typedef struct enc_photon_opts {
+  float light_center[3];
+  float light_size;      /* square light facing -y, side length */
+  uint32_t nphotons;     /* photons emitted; each carries power 1/nphotons per channel */
+  uint32_t max_bounces;  /* m_cMaxBounces: a path makes at most max_bounces + 1 hits */
+  float albedo;          /* diffuse reflectance = Russian roulette survival */
+  uint32_t seed;
+  float emit_offset;     /* origin offset along the direction at emission (0.01 at unit scale) */
+  float bounce_offset;   /* ... after a diffuse bounce (0.001 at unit scale) */
+} enc_photon_opts;
+/* Photon emission and tracing (PhotonMapperCPU::EmitPhotons / TracePhoton /
+ * ReflectPhotonDiffusely, PhotonMapperCPU.cpp:503-745): photons leave the
+ * light in a cosine lobe (RectangleLight::EmitPhoton, RectangleLight.cpp:172-185),
+ * a photon is stored at every surface hit with the hit's stored normal, and
+ * the path continues with probability albedo in a cosine lobe about that
+ * normal.  Stores into the capacity-sized arrays (3 floats per photon);
+ * *stored = photons stored (those past capacity are dropped, as AddPhoton
+ * drops photons into a full map).  Synchronises `stream`. */
+enc_status enc_photons_trace_device(enc_accel accel, const enc_photon_opts* opts, float* d_pos,
+                                    float* d_nrm, float* d_pow, uint32_t capacity,
+                                    uint32_t* stored, enc_stream stream);
+/* PhotonMap over photon arrays in device memory (3 floats each per photon). */
+enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, const float* d_pow,
+                                       size_t nphotons, int32_t caustic, int32_t device,
+                                       enc_photonmap* out);
+
 /* PhotonMap: AddPhoton x n followed by BalanceAndConstruct
  * (PhotonMap.cpp:46-53, 167-221).  caustic != 0 selects the caustic-map
  * estimate (cone weight and N/(pi r^2), PhotonMap.cpp:147, 157). */
