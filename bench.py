@@ -730,14 +730,21 @@ def main():
     ap.add_argument("--stack", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched multi-scene and served sections")
+                    help="skip the batched multi-scene, served and photon-gather sections")
+    ap.add_argument("--gather-only", action="store_true",
+                    help="run only the photon-gather section (prints its JSON object)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up below 3 steps is not a valid measurement; using 3")
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    if args.impl == "reference":
+    if args.gather_only:
+        import torch
+        torch.cuda.set_device(0)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=0)
+        print(json.dumps(gather_section(0, args, flush)), flush=True)
+    elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
         run_engine_arm(args, rank, world)

@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
             tnz = fmaf(u8f(nzs ? qhz : qlz), cz, bz);
             tfz = fmaf(u8f(nzs ? qlz : qhz), cz, bz);
           }
+          // (three-input min/max measured 1.6 % slower here)
           const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
           const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
           const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);

@@ -237,19 +237,23 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
     std::vector<uint8_t> raw(L::kBytes, 0);
     WNodeHeader h;
     std::memset(&h, 0, sizeof(h));
+    // Quantisation grid: origin at the node's lo corner, steps of 2^e with
+    // the node extent in at most 255 of them, and 2^e no finer than the float
+    // spacing at the node (so tiny nodes far from the origin still quantise).
+    // (A grid one step wider on each side, which lets the kernel drop one add
+    // per plane, was measured: the looser boxes cost 7 % more node visits and
+    // more time than the add saves.)
     double scale[3];
     for (int a = 0; a < 3; ++a) {
-      h.p[a] = nb.lo[a];
-      double ext = (double)nb.hi[a] - (double)nb.lo[a];
+      const double ext = (double)nb.hi[a] - (double)nb.lo[a];
+      const float mag = std::max(std::fabs(nb.lo[a]), std::fabs(nb.hi[a]));
+      const double spacing = (double)std::nextafter(mag, INFINITY) - (double)mag;
       int e = -126;
-      if (ext > 0) {
-        e = (int)std::ceil(std::log2(ext / 255.0));
-        while (std::ldexp(255.0, e) < ext) ++e;
-        if (e < -126) e = -126;
-        if (e > 127) throw std::runtime_error("scene extent too large to quantise");
-      }
+      while (std::ldexp(255.0, e) < ext || std::ldexp(1.0, e) < spacing) ++e;
+      if (e > 127) throw std::runtime_error("scene extent too large to quantise");
       h.e[a] = (uint8_t)(e + 127);
       scale[a] = std::ldexp(1.0, e);
+      h.p[a] = nb.lo[a];
     }
     h.nchild = (uint8_t)nk;
     h.child_base = (uint32_t)(queue.size());
@@ -321,8 +325,7 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
       for (int a = 0; a < 3; ++a) {
         double lo = std::floor(((double)c.box.lo[a] - (double)h.p[a]) / scale[a]);
         double hi = std::ceil(((double)c.box.hi[a] - (double)h.p[a]) / scale[a]);
-        lo = std::min(std::max(lo, 0.0), 255.0);
-        hi = std::min(std::max(hi, 0.0), 255.0);
+        if (lo < 0.0 || hi > 255.0) throw std::runtime_error("child box outside its quantisation grid");
         q[a * W + i] = (uint8_t)lo;
         q[(3 + a) * W + i] = (uint8_t)hi;
       }
