@@ -86,6 +86,29 @@ class PhotonOpts(C.Structure):
                 ("seed", C.c_uint32), ("emit_offset", C.c_float), ("bounce_offset", C.c_float)]
 
 
+class ModelXform(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("size", C.c_float), ("angle_deg", C.c_float),
+                ("axis", C.c_float * 3)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("ntris", C.c_uint32), ("nprims", C.c_uint32), ("nmodels", C.c_uint32),
+                ("nmaterials", C.c_uint32), ("nlights", C.c_uint32), ("nspheres", C.c_uint32),
+                ("nunknown", C.c_uint32), ("has_camera", C.c_int32), ("cam_eye", C.c_float * 3),
+                ("cam_look", C.c_float * 3), ("cam_up", C.c_float * 3), ("cam_fov_deg", C.c_float),
+                ("cam_aspect", C.c_float), ("cam_near", C.c_float), ("cam_far", C.c_float),
+                ("background", C.c_float * 4)]
+
+
+ENC_LIGHT_RECT = 0
+ENC_LIGHT_POINT = 1
+
+
+class SceneLight(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("center", C.c_float * 3), ("size", C.c_float),
+                ("color", C.c_float * 3)]
+
+
 P = C.c_void_p
 F = C.POINTER(C.c_float)
 
@@ -96,8 +119,16 @@ SIGNATURES = {
     "enc_device_count": (C.c_int32, [C.POINTER(C.c_int32)]),
     "enc_scene_create": (C.c_int32, [P, C.c_uint32, C.POINTER(P)]),
     "enc_scene_destroy": (C.c_int32, [P]),
+    "enc_scene_load_ply": (C.c_int32, [C.c_char_p, C.POINTER(ModelXform), C.POINTER(P)]),
+    "enc_scene_load_file": (C.c_int32, [C.c_char_p, C.c_char_p, C.POINTER(P)]),
+    "enc_scene_desc_get": (C.c_int32, [P, C.POINTER(SceneDesc)]),
+    "enc_scene_tris": (C.c_int32, [P, P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "enc_scene_prims": (C.c_int32, [P, P, P, C.c_uint32]),
+    "enc_scene_materials": (C.c_int32, [P, P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "enc_scene_lights": (C.c_int32, [P, C.POINTER(SceneLight), C.c_uint32, C.POINTER(C.c_uint32)]),
     "enc_accel_build": (C.c_int32, [P, C.POINTER(BuildOpts), C.c_int32, C.POINTER(P)]),
     "enc_accel_destroy": (C.c_int32, [P]),
+    "enc_accel_refit": (C.c_int32, [P, P, C.c_uint32]),
     "enc_accel_info_get": (C.c_int32, [P, C.POINTER(AccelInfo)]),
     "enc_intersect_closest": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),

@@ -95,6 +95,13 @@ class Accelerator:
         self.ntris = t.shape[0]
         return self
 
+    # AccelerationStructure::update (AccelerationStructure.h:51)
+    def update(self, tris: np.ndarray) -> "Accelerator":
+        """The same triangles at new positions: refit (wide BVH) or rebuild (kd)."""
+        t = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+        check(self.lib.enc_accel_refit(self.handle, ptr(t), t.shape[0]), "enc_accel_refit")
+        return self
+
     def info(self) -> dict:
         i = _lib.AccelInfo()
         check(self.lib.enc_accel_info_get(self.handle, C.byref(i)), "enc_accel_info_get")

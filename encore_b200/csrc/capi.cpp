@@ -14,14 +14,11 @@
 
 #include "engine.h"
 #include "photon.h"
-
-struct enc_scene_s {
-  std::vector<float> verts;
-  uint32_t ntris = 0;
-};
+#include "scene.h"
 
 struct enc_accel_s {
   enc::DevAccel dev;
+  enc::WBVHHost host;  // wide BVH kept on the host for refits
   std::mutex mu;  // serialises the host-buffer forms (shared staging buffers)
   void* d_stage_in = nullptr;
   void* d_stage_out = nullptr;
@@ -182,6 +179,8 @@ enc_status enc_scene_create(const float* tri_verts, uint32_t ntris, enc_scene* o
     return ENC_ERR_OUT_OF_MEMORY;
   }
   s->ntris = ntris;
+  s->desc.ntris = ntris;
+  s->desc.nprims = ntris;
   *out = s;
   return ENC_OK;
 }
@@ -257,6 +256,10 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
       if (e == cudaSuccess) e = upload(&d.d_tri_pos, h.tri_pos.data(), h.tri_pos.size());
       d.node_bytes = h.nodes.size();
       d.tri_bytes = h.tris.size() * sizeof(DevTri);
+      // keep the tree for refits (not the triangle records: refit rewrites them)
+      h.tris.clear();
+      h.tris.shrink_to_fit();
+      a->host = std::move(h);
     } else {
       KdHost h;
       build_kd_reference(scene->verts.data(), scene->ntris, &h);
@@ -300,6 +303,72 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
                    kQueueSlots * sizeof(uint32_t) + 16;
   d.build_seconds = now_s() - t0;
   *out = a;
+  return ENC_OK;
+}
+
+enc_status enc_accel_refit(enc_accel a, const float* tri_verts, uint32_t ntris) {
+  if (!a || !tri_verts) {
+    set_error("enc_accel_refit: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DevAccel& d = a->dev;
+  if (ntris != d.ntris) {
+    set_error("enc_accel_refit: the triangle count must stay the same");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(a->mu);
+  DeviceScope ds(d.device);
+  double t0 = now_s();
+  try {
+    if (d.kind == ENC_ACCEL_WBVH) {
+      refit_wbvh(&a->host, tri_verts, ntris);
+      ENC_CUDA(cudaMemcpy(d.d_nodes, a->host.nodes.data(), a->host.nodes.size(), cudaMemcpyHostToDevice),
+               "refit upload");
+      ENC_CUDA(cudaMemcpy(d.d_tris, a->host.tris.data(), a->host.tris.size() * sizeof(DevTri),
+                          cudaMemcpyHostToDevice),
+               "refit upload");
+      for (int i = 0; i < 3; ++i) {
+        d.lo[i] = a->host.lo[i];
+        d.hi[i] = a->host.hi[i];
+      }
+      a->host.tris.clear();
+      a->host.tris.shrink_to_fit();
+    } else {
+      // Kdtree::update rebuilds (Kdtree.h:138); so does the kd layout here
+      KdHost h;
+      build_kd_reference(tri_verts, ntris, &h);
+      std::vector<DevTri> tris(ntris);
+      make_dev_tris(tri_verts, ntris, nullptr, tris.data());
+      KdNode* nodes = nullptr;
+      uint32_t* items = nullptr;
+      cudaError_t e = upload(&nodes, h.nodes.data(), h.nodes.size());
+      if (e == cudaSuccess) e = upload(&items, h.items.data(), h.items.size());
+      if (e == cudaSuccess)
+        e = cudaMemcpy(d.d_tris, tris.data(), tris.size() * sizeof(DevTri), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        cudaFree(nodes);
+        cudaFree(items);
+        return cuda_fail(e, "refit upload");
+      }
+      cudaFree(d.d_kd);
+      cudaFree(d.d_kd_items);
+      d.d_kd = nodes;
+      d.d_kd_items = items;
+      d.nnodes = (uint32_t)h.nodes.size();
+      d.kd_nitems = (uint32_t)h.items.size();
+      d.node_bytes = h.nodes.size() * sizeof(KdNode) + h.items.size() * sizeof(uint32_t);
+      for (int i = 0; i < 3; ++i) {
+        d.kd_root_lo[i] = h.root_lo[i];
+        d.kd_root_hi[i] = h.root_hi[i];
+        d.lo[i] = h.root_lo[i];
+        d.hi[i] = h.root_hi[i];
+      }
+    }
+  } catch (const std::exception& ex) {
+    set_error(std::string("enc_accel_refit: ") + ex.what());
+    return ENC_ERR_INVALID_ARG;
+  }
+  d.build_seconds = now_s() - t0;
   return ENC_OK;
 }
 

@@ -139,6 +139,7 @@ struct WBVHHost {
   uint32_t nnodes = 0;
   std::vector<DevTri> tris;    // leaf order
   std::vector<uint32_t> tri_pos;  // triangle ID -> position in `tris`
+  std::vector<uint32_t> tri_order;  // position in `tris` -> triangle ID
   float lo[3], hi[3];
   int depth = 0;               // levels of wide nodes (root = 1)
 };
@@ -153,6 +154,9 @@ struct KdHost {
 // Builders (host).  tri_verts: 9 floats per triangle.
 void build_wbvh(const float* tri_verts, uint32_t ntris, int width, int max_leaf, WBVHHost* out);
 void build_kd_reference(const float* tri_verts, uint32_t ntris, KdHost* out);
+// Recomputes the boxes of a built wide BVH for moved triangles (same IDs,
+// same tree shape) and rewrites its triangle records.
+void refit_wbvh(WBVHHost* h, const float* tri_verts, uint32_t ntris);
 void make_dev_tris(const float* tri_verts, uint32_t ntris, const uint32_t* order, DevTri* out);
 
 // Launch parameters after defaults are applied.

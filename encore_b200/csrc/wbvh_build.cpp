@@ -193,6 +193,48 @@ struct BinaryBuilder {
   }
 };
 
+// Writes the node origin, scale exponents and the 8-bit child planes of a
+// wide node: the grid has its origin at the node's lo corner and steps of
+// 2^e with the node extent in at most 255 of them, 2^e no finer than the
+// float spacing at the node (so tiny nodes far from the origin still
+// quantise); each child's lo is rounded down and hi up, so the decoded box
+// contains the child box.  Empty slots get an inverted box (lo 255, hi 0)
+// that no ray enters.  (A grid one step wider on each side, which lets the
+// kernel drop one add per plane, was measured: the looser boxes cost 7 % more
+// node visits and more time than the add saves.)
+template <int W>
+void quantize_node(const Box& nb, const Box* slot_box, const bool* slot_used, WNodeHeader* h,
+                   uint8_t* raw) {
+  using L = WNodeLayout<W>;
+  double scale[3];
+  for (int a = 0; a < 3; ++a) {
+    const double ext = (double)nb.hi[a] - (double)nb.lo[a];
+    const float mag = std::max(std::fabs(nb.lo[a]), std::fabs(nb.hi[a]));
+    const double spacing = (double)std::nextafter(mag, INFINITY) - (double)mag;
+    int e = -126;
+    while (std::ldexp(255.0, e) < ext || std::ldexp(1.0, e) < spacing) ++e;
+    if (e > 127) throw std::runtime_error("scene extent too large to quantise");
+    h->e[a] = (uint8_t)(e + 127);
+    scale[a] = std::ldexp(1.0, e);
+    h->p[a] = nb.lo[a];
+  }
+  uint8_t* q = raw + L::kQOff;
+  for (int i = 0; i < W; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      if (!slot_used[i]) {
+        q[a * W + i] = 255;
+        q[(3 + a) * W + i] = 0;
+        continue;
+      }
+      const double lo = std::floor(((double)slot_box[i].lo[a] - (double)h->p[a]) / scale[a]);
+      const double hi = std::ceil(((double)slot_box[i].hi[a] - (double)h->p[a]) / scale[a]);
+      if (lo < 0.0 || hi > 255.0) throw std::runtime_error("child box outside its quantisation grid");
+      q[a * W + i] = (uint8_t)lo;
+      q[(3 + a) * W + i] = (uint8_t)hi;
+    }
+  }
+}
+
 template <int W>
 void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
               const float* tri_verts, WBVHHost* out) {
@@ -237,24 +279,6 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
     std::vector<uint8_t> raw(L::kBytes, 0);
     WNodeHeader h;
     std::memset(&h, 0, sizeof(h));
-    // Quantisation grid: origin at the node's lo corner, steps of 2^e with
-    // the node extent in at most 255 of them, and 2^e no finer than the float
-    // spacing at the node (so tiny nodes far from the origin still quantise).
-    // (A grid one step wider on each side, which lets the kernel drop one add
-    // per plane, was measured: the looser boxes cost 7 % more node visits and
-    // more time than the add saves.)
-    double scale[3];
-    for (int a = 0; a < 3; ++a) {
-      const double ext = (double)nb.hi[a] - (double)nb.lo[a];
-      const float mag = std::max(std::fabs(nb.lo[a]), std::fabs(nb.hi[a]));
-      const double spacing = (double)std::nextafter(mag, INFINITY) - (double)mag;
-      int e = -126;
-      while (std::ldexp(255.0, e) < ext || std::ldexp(1.0, e) < spacing) ++e;
-      if (e > 127) throw std::runtime_error("scene extent too large to quantise");
-      h.e[a] = (uint8_t)(e + 127);
-      scale[a] = std::ldexp(1.0, e);
-      h.p[a] = nb.lo[a];
-    }
     h.nchild = (uint8_t)nk;
     h.child_base = (uint32_t)(queue.size());
     h.tri_base = (uint32_t)tri_order.size();
@@ -298,17 +322,13 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
     }
     int n_internal = 0;
     uint8_t* meta = raw.data() + L::kMetaOff;
-    uint8_t* q = raw.data() + L::kQOff;
+    Box slot_box[W];
+    bool slot_used[W];
     for (int i = 0; i < W; ++i) {
-      if (slot_child[i] < 0) {
-        // Empty slot: meta 0 and an inverted box (lo 255, hi 0), never hit.
-        for (int a = 0; a < 3; ++a) {
-          q[a * W + i] = 255;
-          q[(3 + a) * W + i] = 0;
-        }
-        continue;
-      }
+      slot_used[i] = slot_child[i] >= 0;
+      if (!slot_used[i]) continue;
       const BNode& c = bn[kids[slot_child[i]]];
+      slot_box[i] = c.box;
       if (c.left >= 0) {
         meta[i] = (uint8_t)(1 + n_internal);
         ++n_internal;
@@ -322,19 +342,14 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
         meta[i] = (uint8_t)((c.count << 5) | off);
         for (uint32_t k = 0; k < c.count; ++k) tri_order.push_back(order[c.first + k]);
       }
-      for (int a = 0; a < 3; ++a) {
-        double lo = std::floor(((double)c.box.lo[a] - (double)h.p[a]) / scale[a]);
-        double hi = std::ceil(((double)c.box.hi[a] - (double)h.p[a]) / scale[a]);
-        if (lo < 0.0 || hi > 255.0) throw std::runtime_error("child box outside its quantisation grid");
-        q[a * W + i] = (uint8_t)lo;
-        q[(3 + a) * W + i] = (uint8_t)hi;
-      }
     }
+    quantize_node<W>(nb, slot_box, slot_used, &h, raw.data());
     std::memcpy(raw.data(), &h, sizeof(h));
     nodes.insert(nodes.end(), raw.begin(), raw.end());
   }
   out->nnodes = (uint32_t)queue.size();
   out->depth = max_level;
+  out->tri_order = tri_order;
   out->tri_pos.assign(tri_order.size(), 0);
   for (size_t i = 0; i < tri_order.size(); ++i) out->tri_pos[tri_order[i]] = (uint32_t)i;
   out->tris.resize(tri_order.size());
@@ -366,16 +381,19 @@ void make_dev_tris(const float* v, uint32_t n, const uint32_t* order, DevTri* ou
   }
 }
 
-void build_wbvh(const float* tri_verts, uint32_t ntris, int width, int max_leaf, WBVHHost* out) {
-  if (ntris == 0) throw std::runtime_error("empty scene");
-  if (max_leaf < 1 || max_leaf > 4) throw std::runtime_error("max_leaf_tris must be 1..4");
-  std::vector<Box> pbox(ntris);
-  std::vector<float> cent(3 * (size_t)ntris);
+namespace {
+
+// Triangle boxes padded by 1e-5 of the larger of the scene extent and the
+// largest coordinate, the scene bounds, and (if asked) the unpadded box
+// centres the SAH bins on.
+std::vector<Box> padded_boxes(const float* v, uint32_t n, float lo[3], float hi[3],
+                              std::vector<float>* cent = nullptr) {
+  std::vector<Box> pbox(n);
   Box scene;
   scene.empty();
   float maxabs = 0.f;
-  for (uint32_t i = 0; i < ntris; ++i) {
-    const float* t = tri_verts + 9 * (size_t)i;
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* t = v + 9 * (size_t)i;
     Box b;
     b.empty();
     b.grow(t);
@@ -385,21 +403,80 @@ void build_wbvh(const float* tri_verts, uint32_t ntris, int width, int max_leaf,
     scene.grow(b);
     for (int k = 0; k < 9; ++k) maxabs = std::max(maxabs, std::fabs(t[k]));
   }
-  for (int a = 0; a < 3; ++a) {
-    out->lo[a] = scene.lo[a];
-    out->hi[a] = scene.hi[a];
-  }
-  float ext = std::max(std::max(scene.hi[0] - scene.lo[0], scene.hi[1] - scene.lo[1]),
-                       scene.hi[2] - scene.lo[2]);
+  const float ext = std::max(std::max(scene.hi[0] - scene.lo[0], scene.hi[1] - scene.lo[1]),
+                             scene.hi[2] - scene.lo[2]);
   float pad = 1e-5f * std::max(ext, maxabs);
   if (!(pad > 0.f)) pad = 1e-30f;
-  for (uint32_t i = 0; i < ntris; ++i) {
+  if (cent) cent->resize(3 * (size_t)n);
+  for (uint32_t i = 0; i < n; ++i)
     for (int a = 0; a < 3; ++a) {
-      cent[3 * (size_t)i + a] = 0.5f * (pbox[i].lo[a] + pbox[i].hi[a]);
+      if (cent) (*cent)[3 * (size_t)i + a] = 0.5f * (pbox[i].lo[a] + pbox[i].hi[a]);
       pbox[i].lo[a] -= pad;
       pbox[i].hi[a] += pad;
     }
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = scene.lo[a];
+    hi[a] = scene.hi[a];
   }
+  return pbox;
+}
+
+// Bottom-up refit: the nodes are in breadth-first order, so every child has
+// a larger index than its parent and one reverse pass sees children first.
+template <int W>
+void refit_w(WBVHHost* H, const float* v, uint32_t ntris) {
+  using L = WNodeLayout<W>;
+  std::vector<Box> pbox = padded_boxes(v, ntris, H->lo, H->hi);
+  std::vector<Box> nbox(H->nnodes);
+  for (int64_t i = (int64_t)H->nnodes - 1; i >= 0; --i) {
+    uint8_t* raw = H->nodes.data() + (size_t)i * L::kBytes;
+    WNodeHeader h;
+    std::memcpy(&h, raw, sizeof(h));
+    const uint8_t* meta = raw + L::kMetaOff;
+    Box slot_box[W];
+    bool used[W];
+    Box nb;
+    nb.empty();
+    for (int c = 0; c < W; ++c) {
+      const uint32_t m = meta[c];
+      used[c] = m != 0;
+      if (!used[c]) continue;
+      if (m < 32) {
+        const uint32_t child = h.child_base + (m - 1);
+        if (child >= H->nnodes) throw std::runtime_error("refit: corrupt node table");
+        slot_box[c] = nbox[child];
+      } else {
+        slot_box[c].empty();
+        for (uint32_t k = 0; k < (m >> 5); ++k) {
+          const uint32_t slot = h.tri_base + (m & 31u) + k;
+          if (slot >= H->tri_order.size()) throw std::runtime_error("refit: corrupt node table");
+          slot_box[c].grow(pbox[H->tri_order[slot]]);
+        }
+      }
+      nb.grow(slot_box[c]);
+    }
+    nbox[(size_t)i] = nb;
+    quantize_node<W>(nb, slot_box, used, &h, raw);
+    std::memcpy(raw, &h, sizeof(h));
+  }
+  H->tris.resize(H->tri_order.size());
+  make_dev_tris(v, (uint32_t)H->tri_order.size(), H->tri_order.data(), H->tris.data());
+}
+
+}  // namespace
+
+void refit_wbvh(WBVHHost* h, const float* tri_verts, uint32_t ntris) {
+  if (ntris != h->tri_order.size()) throw std::runtime_error("refit needs the same triangle count");
+  if (h->width == 2) refit_w<2>(h, tri_verts, ntris);
+  else if (h->width == 4) refit_w<4>(h, tri_verts, ntris);
+  else refit_w<8>(h, tri_verts, ntris);
+}
+
+void build_wbvh(const float* tri_verts, uint32_t ntris, int width, int max_leaf, WBVHHost* out) {
+  if (ntris == 0) throw std::runtime_error("empty scene");
+  if (max_leaf < 1 || max_leaf > 4) throw std::runtime_error("max_leaf_tris must be 1..4");
+  std::vector<float> cent;
+  std::vector<Box> pbox = padded_boxes(tri_verts, ntris, out->lo, out->hi, &cent);
   std::vector<uint32_t> idx(ntris);
   for (uint32_t i = 0; i < ntris; ++i) idx[i] = i;
   std::vector<BNode> bn(2 * (size_t)ntris);

@@ -121,12 +121,75 @@ enc_status enc_device_count(int32_t* count);
 enc_status enc_scene_create(const float* tri_verts, uint32_t ntris, enc_scene* out);
 enc_status enc_scene_destroy(enc_scene scene);
 
+/* Scene front-end: the reference's model and scene-file loaders.
+ *
+ * enc_scene_load_ply = Model::Model(filename, ...) for a .ply file: the mesh
+ * read as Model::loadPLY reads it (Model.cpp:396-482; ascii, each face's
+ * first three indices), then moved by Model::centerModel (Model.cpp:109-173:
+ * scaled so its longest side is `size`, centred on `center`, rotated by
+ * `angle_deg` about `axis`) in the reference's float operation order.  Binary
+ * little/big-endian PLY files are read too (an extension; same face rule).
+ *
+ * enc_scene_load_file = Scene::load + Scene::HandleSceneVariable
+ * (Scene.cpp:78-209): MODEL lines load PLY meshes, RECT_LIGHT adds the fixed
+ * two-triangle ceiling light of RectangleLight (RectangleLight.cpp), SPHERE
+ * takes a primitive index but no triangles (the engine traces triangles
+ * only), CAMERA / MATERIAL / POINT_LIGHT / BACKGROUND_COLOR are recorded, a
+ * token starting with '*' comments out the rest of its line.  Triangles are
+ * in primitive-list order; enc_scene_prims gives, per triangle, the
+ * reference's primitive index (a RECT_LIGHT's two triangles share one) and
+ * material index.  Relative model paths resolve against `model_dir` (NULL =
+ * the working directory, as the reference opens them). */
+typedef struct enc_model_xform {
+  float center[3];
+  float size;
+  float angle_deg;
+  float axis[3];
+} enc_model_xform;
+
+typedef struct enc_scene_desc {
+  uint32_t ntris, nprims, nmodels, nmaterials, nlights, nspheres, nunknown;
+  int32_t has_camera;
+  float cam_eye[3], cam_look[3], cam_up[3];
+  float cam_fov_deg, cam_aspect, cam_near, cam_far;
+  float background[4];
+} enc_scene_desc;
+
+#define ENC_LIGHT_RECT 0
+#define ENC_LIGHT_POINT 1
+typedef struct enc_scene_light {
+  int32_t kind;
+  float center[3];  /* RECT: the quad's centre; POINT: the position */
+  float size;       /* RECT: side length (square in the xz plane); POINT: 0 */
+  float color[3];
+} enc_scene_light;
+
+enc_status enc_scene_load_ply(const char* path, const enc_model_xform* xform, enc_scene* out);
+enc_status enc_scene_load_file(const char* path, const char* model_dir, enc_scene* out);
+enc_status enc_scene_desc_get(enc_scene scene, enc_scene_desc* desc);
+/* Copies up to `cap` triangles (9 floats each); *ntris = the scene's count. */
+enc_status enc_scene_tris(enc_scene scene, float* tri_verts, uint32_t cap, uint32_t* ntris);
+/* Per triangle: primitive index and material index (-1 = default material);
+ * either pointer may be NULL.  Writes min(cap, ntris) entries. */
+enc_status enc_scene_prims(enc_scene scene, int32_t* prim_of_tri, int32_t* material_of_tri,
+                           uint32_t cap);
+/* Materials as MATERIAL lists them: diffuse rgb, specular rgb, ambient rgb,
+ * reflectivity, transparency, refraction index, transmittance (13 floats). */
+enc_status enc_scene_materials(enc_scene scene, float* out13, uint32_t cap, uint32_t* n);
+enc_status enc_scene_lights(enc_scene scene, enc_scene_light* out, uint32_t cap, uint32_t* n);
+
 /* AccelerationStructure::build (AccelerationStructure.h:47).  Builds on the
  * host, uploads to `device`, returns an accelerator resident in HBM.  The
  * scene may be destroyed afterwards. */
 enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t device,
                            enc_accel* out);
 enc_status enc_accel_destroy(enc_accel accel);
+/* AccelerationStructure::update (AccelerationStructure.h:51; Bvh::update,
+ * BVH.cpp:52-121): the same triangles (same count and IDs) at new positions.
+ * A wide BVH keeps its tree shape and gets its boxes recomputed bottom-up and
+ * re-quantised; a kd layout is rebuilt, as Kdtree::update rebuilds
+ * (Kdtree.h:138).  Must not run concurrently with queries on the handle. */
+enc_status enc_accel_refit(enc_accel accel, const float* tri_verts, uint32_t ntris);
 enc_status enc_accel_info_get(enc_accel accel, enc_accel_info* info);
 
 /* AccelerationStructure::intersect (AccelerationStructure.h:63), batched.

@@ -67,6 +67,8 @@ def reference():
         lib.encref_pmap_radiance.argtypes = [P, P, P, C.c_long, C.c_int, C.c_float, P, C.c_int]
         lib.encref_pmap_nearest.argtypes = [P, P, P, C.c_long, C.c_int, C.c_float, P, P, P, C.c_int]
         lib.encref_hardware_threads.restype = C.c_int
+        lib.encref_model_load.restype = C.c_long
+        lib.encref_model_load.argtypes = [C.c_char_p, P, C.c_float, C.c_float, P, P, C.c_long]
         _ref = lib
     return _ref
 
@@ -234,4 +236,17 @@ def ref_occluded(tris, rays, kind=0, nthreads=0):
     out = np.empty(r7.shape[0], np.uint8)
     lib.encref_occluded(h, r7.ctypes.data, r7.shape[0], out.ctypes.data, nthreads)
     lib.encref_scene_destroy(h)
+    return out
+
+
+def ref_model_load(path, center, size, angle, axis):
+    """The reference's Model::load + centerModel on a mesh file: (N, 9) float32
+    in primitive-list order (needs oracle/_ref/libencore_ref.so)."""
+    lib = reference()
+    c = np.ascontiguousarray(center, np.float32)
+    ax = np.ascontiguousarray(axis, np.float32)
+    b = str(path).encode()
+    n = lib.encref_model_load(b, c.ctypes.data, size, angle, ax.ctypes.data, None, 0)
+    out = np.empty((n, 9), np.float32)
+    lib.encref_model_load(b, c.ctypes.data, size, angle, ax.ctypes.data, out.ctypes.data, n)
     return out

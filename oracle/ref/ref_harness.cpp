@@ -34,6 +34,8 @@
 #include "PhotonMap.h"
 #include "Photon.h"
 #include "Color.h"
+#include "Model.h"
+#include "Material.h"
 
 extern bool IGNORE_NORMAL;  // ENCORE/src/renderers/PhotonMap.cpp:23
 
@@ -268,5 +270,32 @@ void encref_pmap_nearest(void* h, const float* qpos, const float* qnrm, long nq,
 }
 
 int encref_hardware_threads(void) { return (int)std::thread::hardware_concurrency(); }
+
+// Model::Model(filename, center, size, angle, axis, material) -> Model::load
+// (Model.cpp:34-107): the reference's loader and centring transform.  Writes
+// up to `cap` triangles (9 floats each, primitive-list order, read back
+// through TrianglePrim::getNewTesselation) and returns the primitive count.
+long encref_model_load(const char* path, const float* center, float size, float angle,
+                       const float* axis, float* out, long cap) {
+  Model m(std::string(path), Point3(center[0], center[1], center[2]), size, angle,
+          Vector3(axis[0], axis[1], axis[2]), Material());
+  std::list<IPrimitive*>& pl = m.getPrimitiveList();
+  long i = 0;
+  for (std::list<IPrimitive*>::iterator p = pl.begin(); p != pl.end(); ++p, ++i) {
+    if (i >= cap) continue;
+    std::list<Triangle*>* ts = (*p)->getNewTesselation();
+    Triangle* t = ts->front();
+    const Vertex* v[3] = {t->getVertex0(), t->getVertex1(), t->getVertex2()};
+    for (int k = 0; k < 3; ++k) {
+      const Point3& c = v[k]->getCoordinates();
+      out[9 * i + 3 * k + 0] = c.X();
+      out[9 * i + 3 * k + 1] = c.Y();
+      out[9 * i + 3 * k + 2] = c.Z();
+    }
+    for (std::list<Triangle*>::iterator q = ts->begin(); q != ts->end(); ++q) delete *q;
+    delete ts;
+  }
+  return (long)pl.size();
+}
 
 }  // extern "C"
