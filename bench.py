@@ -537,7 +537,7 @@ def gather_section(dev: int, args, flush) -> dict:
 def run_engine_arm(args, rank: int, world: int) -> None:
     import torch
     import torch.distributed as dist
-    from encore_b200 import Accelerator, HIT_DTYPE, LaunchConfig
+    from encore_b200 import Accelerator, HIT_DTYPE, LaunchConfig, replicas
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -605,16 +605,12 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     ms_any = timed(anyhit, args.steps)
     acc.check(stream)
 
-    total_ms = sum(ms)
-    if world > 1:
-        tt = torch.tensor([total_ms, sum(ms_any)], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms, any_ms = tt.tolist()
-    else:
-        any_ms = sum(ms_any)
+    # whole-job rate: every replica's rays over the slowest replica's device time
+    rate, total_ms = replicas.aggregate_rate(n, args.steps, sum(ms))
+    any_rate, _ = replicas.aggregate_rate(n, args.steps, sum(ms_any))
     ms_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms * 1e-3) / 1e6
-    any_value = world * n * args.steps / (any_ms * 1e-3) / 1e6
+    value = rate / 1e6
+    any_value = any_rate / 1e6
 
     # parity spot check of the timed output against the untimed host-form call
     got = d_hits.cpu().numpy()
@@ -654,12 +650,8 @@ def run_engine_arm(args, rank: int, world: int) -> None:
         t1 = time.perf_counter()
         acc.intersect(h_rays_np, launch=launch, stream=stream, out=h_hits_np)
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = tt.item()
-    e2e_value = world * n * args.steps / (e2e_total * 1e-3) / 1e6
+    e2e_rate, _ = replicas.aggregate_rate(n, args.steps, sum(e2e_ms))
+    e2e_value = e2e_rate / 1e6
     assert np.array_equal(h_hits_np["tri"], hits_ref["tri"])
 
     cpu = None
