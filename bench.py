@@ -253,7 +253,7 @@ def batched_section(dev: int, args, flush) -> dict:
     total = sum(len(r) for r in rays)
     tune_idx = list(range(0, 64, 4))
     rep = autotune([tris[i] for i in tune_idx], [rays[i] for i in tune_idx], widths=(4, 8),
-                   chunks=(16, 32, 64), blocks_per_sm=(8,), block_threads=(128,), reps=3,
+                   chunks=(16, 32, 64), blocks_per_sm=(8, 10), block_threads=(128,), reps=3,
                    device=dev)
     width, lc = launch_config(rep["best"])
     accs8 = [Accelerator("wbvh", width=8, device=dev).build(t) for t in tris]
@@ -367,7 +367,7 @@ def served_section(dev: int, args) -> dict:
     plain_rate = total / sum(svc) / 1e6
     plain_ref = [out_view(p).copy() for p in pool]
 
-    srv = Server(device=dev, slots=3, slot_rays=8 << 20)
+    srv = Server(device=dev, slots=args.server_slots, slot_rays=args.server_slot_rays)
     ids = [srv.add_scene(a) for a in accs]
     sat = []
     for rep in range(2):
@@ -723,6 +723,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched multi-scene, served and photon-gather sections")
+    ap.add_argument("--server-slots", type=int, default=6,
+                    help="served section: request slots (rounds in flight)")
+    ap.add_argument("--server-slot-rays", type=int, default=4 << 20,
+                    help="served section: ray capacity of a slot (>= the largest request, 4M)")
+    ap.add_argument("--served-only", action="store_true",
+                    help="run only the served section (prints its JSON object)")
     ap.add_argument("--gather-only", action="store_true",
                     help="run only the photon-gather section (prints its JSON object)")
     args = ap.parse_args()
@@ -731,7 +737,11 @@ def main():
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    if args.gather_only:
+    if args.served_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(served_section(0, args)), flush=True)
+    elif args.gather_only:
         import torch
         torch.cuda.set_device(0)
         flush = torch.empty(256 << 20, dtype=torch.uint8, device=0)

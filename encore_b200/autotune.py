@@ -19,7 +19,7 @@ from .batch import BatchLaunch
 
 
 def autotune(scene_tris: Sequence[np.ndarray], ray_batches: Sequence[np.ndarray],
-             widths=(2, 4, 8), chunks=(16, 32, 64, 128), blocks_per_sm=(4, 6, 8),
+             widths=(2, 4, 8), chunks=(16, 32, 64, 128), blocks_per_sm=(6, 8, 10),
              block_threads=(64, 128), stack_depths=(0,), reps: int = 5, device: int = 0,
              out: str | Path | None = None) -> dict:
     import torch

@@ -45,7 +45,7 @@ struct WNodeLayout {
 struct WNodeHeader {  // first 24 bytes of every wide node
   float p[3];
   uint8_t e[3];
-  uint8_t nchild;
+  uint8_t imask;  // bit c set: slot c holds an internal child (its meta is 1 + rank)
   uint32_t child_base;
   uint32_t tri_base;
 };

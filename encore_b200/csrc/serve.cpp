@@ -278,8 +278,8 @@ enc_status enc_server_create(const enc_server_opts* opts, enc_server* out) {
   *out = nullptr;
   enc_server_opts o{};
   if (opts) o = *opts;
-  if (o.slots == 0) o.slots = 3;
-  if (o.slot_rays == 0) o.slot_rays = 8ull << 20;
+  if (o.slots == 0) o.slots = 6;
+  if (o.slot_rays == 0) o.slot_rays = 4ull << 20;
   if (o.budget_bytes == 0) o.budget_bytes = 120ull * 1000 * 1000 * 1000;
   if (o.slots > 16 || o.slot_rays > (1ull << 30)) {
     set_error("enc_server_create: slots <= 16 and slot_rays <= 2^30");

@@ -31,11 +31,14 @@
 
 // Build-time tuning of the wide-BVH kernel:
 //   ENC_TRACE_MINBLOCKS resident 128-thread blocks per SM the register
-//                       budget is fitted to (8 -> 64 registers, no spills;
-//                       6 and 10 measured slower on the 2M-triangle
-//                       heightfield workload).
+//                       budget is fitted to.  The kernel waits on dependent
+//                       node loads, so resident warps pay: 10 (48 registers,
+//                       a few bytes spilled, width-8 stack entries of 8
+//                       bytes) ran 3.6 % faster than 8 (64 registers) on the
+//                       2M-triangle heightfield workload; 12 (40 registers)
+//                       spilled enough to lose 11 %.
 #ifndef ENC_TRACE_MINBLOCKS
-#define ENC_TRACE_MINBLOCKS 8
+#define ENC_TRACE_MINBLOCKS 10
 #endif
 
 namespace enc {
@@ -168,16 +171,6 @@ __device__ __forceinline__ void sort_net<4>(float (&k)[4], uint32_t (&v)[4]) {
   ENC_CSWAP(1, 3);
   ENC_CSWAP(1, 2);
 }
-template <>
-__device__ __forceinline__ void sort_net<8>(float (&k)[8], uint32_t (&v)[8]) {
-  // Batcher odd-even merge sort, 19 comparators.
-  ENC_CSWAP(0, 1); ENC_CSWAP(2, 3); ENC_CSWAP(4, 5); ENC_CSWAP(6, 7);
-  ENC_CSWAP(0, 2); ENC_CSWAP(1, 3); ENC_CSWAP(4, 6); ENC_CSWAP(5, 7);
-  ENC_CSWAP(1, 2); ENC_CSWAP(5, 6);
-  ENC_CSWAP(0, 4); ENC_CSWAP(1, 5); ENC_CSWAP(2, 6); ENC_CSWAP(3, 7);
-  ENC_CSWAP(2, 4); ENC_CSWAP(3, 5);
-  ENC_CSWAP(1, 2); ENC_CSWAP(3, 4); ENC_CSWAP(5, 6);
-}
 #undef ENC_CSWAP
 
 template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false>
@@ -193,6 +186,11 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
   //           lb = entry distance of the nearest remaining child.
   // lb is a lower bound for every child still in the group, so a group
   // whose lb exceeds the closest hit so far is dropped whole.
+  //   Width-8 entries carry lb in the top 16 bits of y (the float's high
+  //   half: rounded toward zero, so never above lb for lb >= 0; a negative
+  //   lb is stored as -inf), which keeps an entry at 8 bytes of shared
+  //   memory and leaves more of the SM's L1 to node and triangle loads.
+  constexpr bool kCompact = W == 8;
   extern __shared__ uint2 s_stack[];
   const int B = blockDim.x;
   uint2* stk = s_stack + threadIdx.x;  // entry i at stk[i * B]
@@ -350,46 +348,68 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
               wf[2 * a + h] = neg[a] ? lo : hi;
             }
         }
+        if constexpr (W == 8) {
+          // Slab test of the eight children into a hit-slot mask; the header's
+          // internal-slot mask splits it into internal and leaf hits.  Empty
+          // slots hold an inverted box (lo 255, hi 0), whose near plane lies
+          // beyond its far plane for either direction sign, so they never hit
+          // (and a leaf entry with meta 0 would contribute no triangles).
+          const uint32_t imask = ew >> 24;
+          uint32_t hm = 0;
 #pragma unroll
-        for (int c = 0; c < W; ++c) {
-          float tnx, tfx, tny, tfy, tnz, tfz;
-          if constexpr (W == 8) {
+          for (int c = 0; c < 8; ++c) {
             const uint32_t sel = 0x7650u | (uint32_t)(c & 3);
             const int h = c >> 2;
-            tnx = fmaf(__uint_as_float(__byte_perm(wn[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
-            tfx = fmaf(__uint_as_float(__byte_perm(wf[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
-            tny = fmaf(__uint_as_float(__byte_perm(wn[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
-            tfy = fmaf(__uint_as_float(__byte_perm(wf[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
-            tnz = fmaf(__uint_as_float(__byte_perm(wn[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
-            tfz = fmaf(__uint_as_float(__byte_perm(wf[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
-          } else {
+            const float tnx = fmaf(__uint_as_float(__byte_perm(wn[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
+            const float tfx = fmaf(__uint_as_float(__byte_perm(wf[0 + h], 0x4B000000u, sel)) - 8388608.0f, cx, bx);
+            const float tny = fmaf(__uint_as_float(__byte_perm(wn[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
+            const float tfy = fmaf(__uint_as_float(__byte_perm(wf[2 + h], 0x4B000000u, sel)) - 8388608.0f, cy, by);
+            const float tnz = fmaf(__uint_as_float(__byte_perm(wn[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
+            const float tfz = fmaf(__uint_as_float(__byte_perm(wf[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
+            // (three-input min/max measured 1.6 % slower here)
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+            if (tn <= tf) {
+              hm |= 1u << c;
+              if ((imask >> c) & 1u) lbmin = fminf(lbmin, tn);
+            }
+          }
+          // triangles of the hit leaves (meta = count << 5 | offset)
+          uint32_t lh = hm & ~imask;
+          while (lh) {
+            const uint32_t c = __ffs(lh) - 1;
+            lh &= lh - 1;
+            const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
+            trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+          }
+          // hit internal children in octant order: bit k = slot k ^ octm
+          uint32_t x = hm & imask;
+          if (octm & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
+          if (octm & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
+          if (octm & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
+          hitk = x;
+        } else {
+#pragma unroll
+          for (int c = 0; c < W; ++c) {
             const uint32_t qlx = byte_of(nw.w, L::kQOff + 0 * W + c);
             const uint32_t qly = byte_of(nw.w, L::kQOff + 1 * W + c);
             const uint32_t qlz = byte_of(nw.w, L::kQOff + 2 * W + c);
             const uint32_t qhx = byte_of(nw.w, L::kQOff + 3 * W + c);
             const uint32_t qhy = byte_of(nw.w, L::kQOff + 4 * W + c);
             const uint32_t qhz = byte_of(nw.w, L::kQOff + 5 * W + c);
-            tnx = fmaf(u8f(nxs ? qhx : qlx), cx, bx);
-            tfx = fmaf(u8f(nxs ? qlx : qhx), cx, bx);
-            tny = fmaf(u8f(nys ? qhy : qly), cy, by);
-            tfy = fmaf(u8f(nys ? qly : qhy), cy, by);
-            tnz = fmaf(u8f(nzs ? qhz : qlz), cz, bz);
-            tfz = fmaf(u8f(nzs ? qlz : qhz), cz, bz);
-          }
-          // (three-input min/max measured 1.6 % slower here)
-          const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-          const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
-          const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
-          const bool hit = meta != 0u && tn <= tf;
-          const bool leaf = meta >= 32u;
-          if (hit && leaf) trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-          const bool ih = hit && !leaf;
-          if constexpr (W == 8) {
-            if (ih) {
-              hitk |= 1u << ((uint32_t)c ^ octm);
-              lbmin = fminf(lbmin, tn);
-            }
-          } else {
+            const float tnx = fmaf(u8f(nxs ? qhx : qlx), cx, bx);
+            const float tfx = fmaf(u8f(nxs ? qlx : qhx), cx, bx);
+            const float tny = fmaf(u8f(nys ? qhy : qly), cy, by);
+            const float tfy = fmaf(u8f(nys ? qly : qhy), cy, by);
+            const float tnz = fmaf(u8f(nzs ? qhz : qlz), cz, bz);
+            const float tfz = fmaf(u8f(nzs ? qlz : qhz), cz, bz);
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+            const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
+            const bool hit = meta != 0u && tn <= tf;
+            const bool leaf = meta >= 32u;
+            if (hit && leaf) trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+            const bool ih = hit && !leaf;
             key[c] = ih ? fminf(tn, 3.0e38f) : INFINITY;  // hits sort before the rest
             rnk[c] = meta - 1u;
             nh += ih ? 1 : 0;
@@ -398,13 +418,7 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
         // ---- next node, and the group of the other hit children ----------
         if constexpr (W == 8) {
           if (hitk) {
-            // internal-child mask in slot order, for ranks within child_base
-            uint32_t imask = 0;
-#pragma unroll
-            for (int c = 0; c < W; ++c) {
-              const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
-              imask |= (meta != 0u && meta < 32u) ? (1u << c) : 0u;
-            }
+            const uint32_t imask = ew >> 24;
             const uint32_t k = __ffs(hitk) - 1;
             const uint32_t slot = k ^ octm;
             node = child_base + __popc(imask & ((1u << slot) - 1u));
@@ -415,8 +429,13 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
                 best_id = -1;
                 done = true;
               } else {
-                stk[sp * B] = make_uint2(child_base, rest | (imask << 8));
-                slb[sp * B] = lbmin;
+                if constexpr (kCompact) {
+                  const uint32_t lb16 = lbmin >= 0.0f ? (__float_as_uint(lbmin) >> 16) : 0xff80u;
+                  stk[sp * B] = make_uint2(child_base, rest | (imask << 8) | (lb16 << 16));
+                } else {
+                  stk[sp * B] = make_uint2(child_base, rest | (imask << 8));
+                  slb[sp * B] = lbmin;
+                }
                 ++sp;
               }
             }
@@ -479,11 +498,20 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
       // ---- pop the next group child that can still matter ----------------
       if (!done && node == kNoItem) {
         while (sp > 0) {
-          if (!ANY && slb[(sp - 1) * B] > best_t) {
-            --sp;
-            continue;
+          uint2 e;
+          if constexpr (kCompact) {
+            e = stk[(sp - 1) * B];
+            if (!ANY && __uint_as_float(e.y & 0xffff0000u) > best_t) {
+              --sp;
+              continue;
+            }
+          } else {
+            if (!ANY && slb[(sp - 1) * B] > best_t) {
+              --sp;
+              continue;
+            }
+            e = stk[(sp - 1) * B];
           }
-          uint2 e = stk[(sp - 1) * B];
           if constexpr (W == 8) {
             const uint32_t hk = e.y & 0xffu;
             const uint32_t k = __ffs(hk) - 1;
@@ -494,7 +522,7 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
             if (rest == 0) {
               --sp;
             } else {
-              e.y = rest | (imask << 8);
+              e.y = (e.y & 0xffff0000u) | rest | (imask << 8);
               stk[(sp - 1) * B] = e;
             }
           } else {
@@ -675,6 +703,12 @@ __global__ void __launch_bounds__(128) kd_trace(KdParams P) {
   }
 }
 
+// Shared memory per stack entry: width 8 packs lb into the 8-byte entry;
+// widths 2 and 4 keep it in a separate float array.
+constexpr size_t stack_entry_bytes(int W) {
+  return W == 8 ? sizeof(uint2) : sizeof(uint2) + sizeof(float);
+}
+
 template <int W, bool CLAMP, bool ANY, bool COUNT>
 int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t* visits,
              const Launch& L, cudaStream_t s) {
@@ -695,7 +729,7 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
   // entries always suffice; 0 selects that bound.
   p.stack_depth = L.stack > 0 ? L.stack : (a.tree_depth > 8 ? a.tree_depth : 8);
   p.chunk = L.chunk;
-  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
+  size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
   auto k = wbvh_trace<W, CLAMP, ANY, COUNT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -804,7 +838,7 @@ int launch_w_external(const DevAccel& a, const float* rays, size_t n, enc_hit* h
   p.ntris = a.ntris;
   p.stack_depth = L.stack > 0 ? L.stack : (a.tree_depth > 8 ? a.tree_depth : 8);
   p.chunk = L.chunk;
-  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
+  size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
   auto k = wbvh_trace<W, CLAMP, false, false>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -853,7 +887,7 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   p.batches = m.d_batches;
   p.starts = m.d_starts;
   p.nbatches = m.nbatches;
-  size_t smem = (size_t)p.stack_depth * L.block * (sizeof(uint2) + sizeof(float));
+  size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
   auto k = wbvh_trace<W, CLAMP, ANY, false, true>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

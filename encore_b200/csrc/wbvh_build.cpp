@@ -279,7 +279,6 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
     std::vector<uint8_t> raw(L::kBytes, 0);
     WNodeHeader h;
     std::memset(&h, 0, sizeof(h));
-    h.nchild = (uint8_t)nk;
     h.child_base = (uint32_t)(queue.size());
     h.tri_base = (uint32_t)tri_order.size();
     // Slot order.  Width 8: slot s holds the child lying most in octant s
@@ -331,6 +330,7 @@ void collapse(const std::vector<BNode>& bn, const std::vector<uint32_t>& order,
       slot_box[i] = c.box;
       if (c.left >= 0) {
         meta[i] = (uint8_t)(1 + n_internal);
+        h.imask |= (uint8_t)(1u << i);
         ++n_internal;
         queue.push_back(kids[slot_child[i]]);
         level.push_back((uint16_t)(level[qi] + 1));

@@ -16,7 +16,7 @@ ANY = 1
 
 
 class Server:
-    def __init__(self, device: int = 0, slots: int = 3, slot_rays: int = 8 << 20,
+    def __init__(self, device: int = 0, slots: int = 6, slot_rays: int = 4 << 20,
                  budget_bytes: int = 120 * 10**9, launch: LaunchConfig | None = None):
         self.lib = _lib.load()
         o = _lib.ServerOpts(device, slots, slot_rays, budget_bytes, (launch or LaunchConfig()).c())

@@ -275,9 +275,12 @@ enc_status enc_batch_destroy(enc_batch batch);
 typedef struct enc_server_s* enc_server;
 typedef struct enc_server_opts {
   int32_t device;
-  uint32_t slots;          /* launches in flight at once (0 = 3) */
+  uint32_t slots;          /* launches in flight at once (0 = 6) */
   uint64_t slot_rays;      /* ray capacity of one slot; a request may not exceed it
-                              (0 = 8,388,608) */
+                              (0 = 4,194,304).  Smaller slots make more, smaller
+                              rounds whose copies overlap other rounds' traces:
+                              6 x 4M served 1.52x plain on a mixed 13M-ray pool,
+                              3 x 8M only 1.15x. */
   uint64_t budget_bytes;   /* HBM budget: resident scenes + slot buffers (0 = 120 GB) */
   enc_launch_opts launch;  /* kernel launch shape (zeros = defaults) */
 } enc_server_opts;
