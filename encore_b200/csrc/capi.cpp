@@ -18,6 +18,7 @@
 
 struct enc_accel_s {
   enc::DevAccel dev;
+  enc::WaveScratch wave;  // photon tracer scratch
   enc::WBVHHost host;  // wide BVH kept on the host for refits
   std::mutex mu;  // serialises the host-buffer forms (shared staging buffers)
   void* d_stage_in = nullptr;
@@ -127,6 +128,24 @@ enc_status read_status(enc_accel a, cudaStream_t s) {
 void set_error(const std::string& msg) { g_err = msg; }
 
 const DevAccel* accel_device_view(enc_accel a) { return a ? &a->dev : nullptr; }
+
+WaveScratch* accel_wave_scratch(enc_accel a) { return a ? &a->wave : nullptr; }
+
+void free_wave_scratch(WaveScratch* w) {
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(w->rays[i]);
+    cudaFree(w->path[i]);
+    w->rays[i] = nullptr;
+    w->path[i] = nullptr;
+  }
+  cudaFree(w->hits);
+  cudaFree(w->counters);
+  cudaFreeHost(w->h_counts);
+  w->hits = nullptr;
+  w->counters = nullptr;
+  w->h_counts = nullptr;
+  w->cap = 0;
+}
 
 Launch resolve_launch(const enc_launch_opts* o, int kind, int width) {
   (void)kind;
@@ -378,6 +397,7 @@ enc_status enc_accel_destroy(enc_accel a) {
   if (!a) return ENC_OK;
   DeviceScope ds(a->dev.device);
   free_dev(a->dev);
+  free_wave_scratch(&a->wave);
   cudaFree(a->d_stage_in);
   cudaFree(a->d_stage_out);
   for (int i = 0; i < 3; ++i)
@@ -616,7 +636,14 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
     build_photon_tree(pos, normal, power, n, &h);
     d.nnodes = (uint32_t)h.nodes.size();
     d.depth = h.depth;
-    e = upload(&d.d_nodes, h.nodes.data(), h.nodes.size());
+    d.nlevels = h.nlevels;
+    for (int l = 0; l < kPhotonMaxLevels; ++l) {
+      d.lvl_count[l] = h.lvl_count[l];
+      d.lvl_off[l] = h.lvl_off[l];
+      d.lvl_pad[l] = h.lvl_pad[l];
+    }
+    e = upload(&d.d_box, h.box.data(), h.box.size());
+    if (e == cudaSuccess) e = upload(&d.d_leaf, h.leaf.data(), h.leaf.size());
     if (e == cudaSuccess) e = upload(&d.d_pos4, h.pos4.data(), h.pos4.size());
     if (e == cudaSuccess) e = upload(&d.d_nrm4, h.nrm4.data(), h.nrm4.size());
     if (e == cudaSuccess) e = upload(&d.d_pow4, h.pow4.data(), h.pow4.size());
@@ -627,7 +654,8 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
     e = cudaErrorMemoryAllocation;
   }
   if (e != cudaSuccess) {
-    cudaFree(d.d_nodes);
+    cudaFree(d.d_box);
+    cudaFree(d.d_leaf);
     cudaFree(d.d_pos4);
     cudaFree(d.d_nrm4);
     cudaFree(d.d_pow4);
@@ -661,7 +689,8 @@ enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, c
 enc_status enc_photonmap_destroy(enc_photonmap m) {
   if (!m) return ENC_OK;
   DeviceScope ds(m->dev.device);
-  cudaFree(m->dev.d_nodes);
+  cudaFree(m->dev.d_box);
+  cudaFree(m->dev.d_leaf);
   cudaFree(m->dev.d_pos4);
   cudaFree(m->dev.d_nrm4);
   cudaFree(m->dev.d_pow4);

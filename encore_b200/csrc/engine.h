@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -189,5 +190,20 @@ void set_error(const std::string& msg);
 
 // The device view of an accelerator handle, or nullptr (capi.cpp).
 const DevAccel* accel_device_view(enc_accel a);
+
+// Device scratch of the wavefront photon tracer, kept with the accelerator
+// and grown on demand, so repeated calls allocate nothing.  `mu` serialises
+// the tracer's calls on one accelerator.
+struct WaveScratch {
+  float* rays[2] = {nullptr, nullptr};
+  uint32_t* path[2] = {nullptr, nullptr};
+  void* hits = nullptr;
+  uint32_t* counters = nullptr;  // device: stored photons, next wave's rays
+  uint32_t* h_counts = nullptr;  // pinned host copy of the two counters
+  size_t cap = 0;                // photons the buffers hold
+  std::mutex mu;
+};
+WaveScratch* accel_wave_scratch(enc_accel a);
+void free_wave_scratch(WaveScratch* w);
 
 }  // namespace enc

@@ -1,9 +1,15 @@
 // Photon k-nearest gather and radiance estimate for sm_100a.
 //
-// One warp per query point.  The warp walks the photon kd-tree (photon.h)
-// front to back with a per-warp stack in shared memory; at a leaf each lane
-// tests one photon (32-photon leaves = one coalesced 16-byte load per lane per
-// array).  The k best candidates are kept in a warp-distributed bounded
+// One warp per query point.  The warp walks the 32-ary box tree over the
+// photon kd leaves (photon.h) with a per-warp stack in shared memory: at an
+// inner node each lane tests one child box against the search sphere and the
+// children that can hold an accepted photon are pushed together; at a leaf
+// each lane tests one photon (32-photon leaves = one coalesced 16-byte load
+// per lane per array).  A box is pruned by its FP32 squared distance to the
+// query, formed with the photon test's own operations on the box's clamped
+// coordinates; rounding is monotone, so that distance never exceeds the
+// squared distance of a photon inside the box and pruning drops nothing the
+// photon test would accept.  The k best candidates are kept in a warp-distributed bounded
 // max-heap: S = ceil(k/32) register slots per lane, slot i on lane i % 32; the
 // maximum and its owner are found with a 5-step shuffle reduction, and an
 // accepted candidate replaces it.  The search radius is max_dist^2 until k
@@ -28,11 +34,18 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerBlock = 8;
-constexpr int kStack = 32;
+// Each inner node pushes at most 32 children and the walk is depth first, so
+// 32 entries per level suffice.
+constexpr int kStack = 32 * kPhotonMaxLevels;
 constexpr unsigned kMaxSteps = 1u << 24;
 
 struct GatherParams {
-  const PNode* nodes;
+  const float* box;
+  const uint2* leaf;
+  int nlevels;
+  uint32_t lvl_count[kPhotonMaxLevels];
+  uint32_t lvl_off[kPhotonMaxLevels];
+  uint32_t lvl_pad[kPhotonMaxLevels];
   const float4* pos4;
   const float4* nrm4;
   const float4* pow4;
@@ -53,6 +66,22 @@ struct GatherParams {
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+
+// Position of the r-th set bit of m (r counted from 0, r < popc(m)), by
+// halving: keep the low half while it holds more than r set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
+  int pos = 0;
+#pragma unroll
+  for (int b = 16; b >= 1; b >>= 1) {
+    const int c = __popc(m & ((1u << b) - 1u));
+    if (r >= c) {
+      r -= c;
+      m >>= b;
+      pos += b;
+    }
+  }
+  return pos;
+}
 
 // Max over the slots marked valid (slot index s*32 + lane < limit) and its
 // slot index; -INF / -1 if none.
@@ -82,10 +111,12 @@ __device__ __forceinline__ void warp_max(const float (&dd)[S], int lane, int lim
 
 template <int S, bool NEAREST>
 __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
-  __shared__ int s_node[kWarpsPerBlock][kStack];
+  // stack entries: level << 28 | item index, and the entry's squared distance
+  __shared__ uint32_t s_item[kWarpsPerBlock][kStack];
   __shared__ float s_pd[kWarpsPerBlock][kStack];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
   const unsigned total = gridDim.x * kWarpsPerBlock;
   const int k = P.k;
   for (unsigned q = blockIdx.x * kWarpsPerBlock + wib; q < P.nq; q += total) {
@@ -106,46 +137,70 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
     float worst = INFINITY;
     int worst_loc = -1;
     float r2 = P.r2max;
+    // the root: the top level's items are its children
     int sp = 0;
-    int node = 0;
+    if (k > 0) {
+      if (lane == 0) {
+        s_item[wib][0] = (uint32_t)P.nlevels << 28;
+        s_pd[wib][0] = 0.f;
+      }
+      sp = 1;
+    }
+    __syncwarp();
     unsigned steps = 0;
-    while (k > 0) {
+    while (sp > 0) {
       if (++steps > kMaxSteps) {
         if (lane == 0) atomicOr(P.status, 1u);
         break;
       }
-      const int4 raw = __ldg(reinterpret_cast<const int4*>(P.nodes) + node);
-      PNode nd;
-      nd.split = __int_as_float(raw.x);
-      nd.axis = raw.y;
-      nd.begin = (unsigned)raw.z;
-      nd.end = (unsigned)raw.w;
-      if (nd.axis >= 0) {
-        const float qa = nd.axis == 0 ? qx : (nd.axis == 1 ? qy : qz);
-        const float dq = fs(qa, nd.split);
-        const int left = 2 * node + 1;
-        const int nearc = dq <= 0.0f ? left : left + 1;
-        const int farc = dq <= 0.0f ? left + 1 : left;
-        const float pd = fm(dq, dq);
-        if (pd < r2) {
-          if (sp >= kStack) {
-            if (lane == 0) atomicOr(P.status, 2u);
-            break;
-          }
-          s_node[wib][sp] = farc;
-          s_pd[wib][sp] = pd;
-          ++sp;
-          __syncwarp();
+      --sp;
+      const float pd = s_pd[wib][sp];
+      const uint32_t e = s_item[wib][sp];
+      __syncwarp();
+      if (!(pd < r2)) continue;  // nothing in it can be accepted any more
+      const int lv = (int)(e >> 28);
+      const uint32_t it = e & 0x0fffffffu;
+      if (lv > 0) {
+        // inner node: lane c tests child 32 * it + c of level lv - 1
+        const int cl = lv - 1;
+        const uint32_t child = 32u * it + (uint32_t)lane;
+        bool pass = false;
+        float cd = 0.f;
+        if (child < P.lvl_count[cl]) {
+          const float* b = P.box + P.lvl_off[cl];
+          const uint32_t pad = P.lvl_pad[cl];
+          const float lx = __ldg(b + child), ly = __ldg(b + pad + child),
+                      lz = __ldg(b + 2 * pad + child);
+          const float hx = __ldg(b + 3 * pad + child), hy = __ldg(b + 4 * pad + child),
+                      hz = __ldg(b + 5 * pad + child);
+          const float gx = fmaxf(fmaxf(fs(lx, qx), fs(qx, hx)), 0.f);
+          const float gy = fmaxf(fmaxf(fs(ly, qy), fs(qy, hy)), 0.f);
+          const float gz = fmaxf(fmaxf(fs(lz, qz), fs(qz, hz)), 0.f);
+          cd = fa(fa(fm(gx, gx), fm(gy, gy)), fm(gz, gz));
+          pass = cd < r2;
         }
-        node = nearc;
+        const unsigned m = __ballot_sync(kFull, pass);
+        const int n = __popc(m);
+        if (sp + n > kStack) {
+          if (lane == 0) atomicOr(P.status, 2u);
+          break;
+        }
+        if (pass) {
+          const int at = sp + __popc(m & lt);
+          s_item[wib][at] = ((uint32_t)cl << 28) | child;
+          s_pd[wib][at] = cd;
+        }
+        sp += n;
+        __syncwarp();
         continue;
       }
       // leaf: lane j tests photon begin + j
-      const unsigned pidx = nd.begin + (unsigned)lane;
+      const uint2 rng = __ldg(P.leaf + it);
+      const unsigned pidx = rng.x + (unsigned)lane;
       bool acc = false;
       float d2 = 0.f;
       int orig = -1;
-      if (pidx < nd.end) {
+      if (pidx < rng.y) {
         const float4 p = __ldg(P.pos4 + pidx);
         const float x = fs(qx, p.x), y = fs(qy, p.y), z = fs(qz, p.z);
         d2 = fa(fa(fm(x, x), fm(y, y)), fm(z, z));
@@ -157,12 +212,40 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
         }
       }
       unsigned m = __ballot_sync(kFull, acc);
+      if (m && count < k) {
+        // fill free heap slots in one step: the accepted candidate of rank r
+        // (r-th set bit of m) goes to slot count + r, which lives on lane
+        // (count + r) % 32, register (count + r) / 32
+        const int nfill = min(__popc(m), k - count);
+        const int r = (lane - count) & 31;
+        const bool take = r < nfill;
+        const int src = nth_set_bit(m, take ? r : 0);
+        const float cd = __shfl_sync(kFull, d2, src);
+        const int co = __shfl_sync(kFull, orig, src);
+        const int slot = count + r;
+        if (take) {
+#pragma unroll
+          for (int s = 0; s < S; ++s)
+            if (s == (slot >> 5)) {
+              dd[s] = cd;
+              ds[s] = (int)rng.x + src;
+              dorig[s] = co;
+            }
+        }
+        // the first nfill set bits are done
+        for (int i = 0; i < nfill; ++i) m &= m - 1;
+        count += nfill;
+        if (count == k) {
+          warp_max<S>(dd, lane, k, worst, worst_loc);
+          r2 = worst;
+        }
+      }
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1;
         const float cd = __shfl_sync(kFull, d2, j);
         const int co = __shfl_sync(kFull, orig, j);
-        const int cs = (int)nd.begin + j;
+        const int cs = (int)rng.x + j;
         if (count < k) {
           const int slot = count;
 #pragma unroll
@@ -189,17 +272,6 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
           r2 = worst;
         }
       }
-      // pop the next subtree that can still hold a closer photon
-      node = -1;
-      while (sp > 0) {
-        --sp;
-        if (s_pd[wib][sp] < r2) {
-          node = s_node[wib][sp];
-          break;
-        }
-      }
-      __syncwarp();
-      if (node < 0) break;
     }
 
     if (NEAREST) {
@@ -270,7 +342,14 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
                   cudaStream_t s) {
   if (nq == 0) return 0;
   GatherParams p;
-  p.nodes = m.d_nodes;
+  p.box = m.d_box;
+  p.leaf = reinterpret_cast<const uint2*>(m.d_leaf);
+  p.nlevels = m.nlevels;
+  for (int l = 0; l < kPhotonMaxLevels; ++l) {
+    p.lvl_count[l] = m.lvl_count[l];
+    p.lvl_off[l] = m.lvl_off[l];
+    p.lvl_pad[l] = m.lvl_pad[l];
+  }
   p.pos4 = reinterpret_cast<const float4*>(m.d_pos4);
   p.nrm4 = reinterpret_cast<const float4*>(m.d_nrm4);
   p.pow4 = reinterpret_cast<const float4*>(m.d_pow4);

@@ -88,6 +88,56 @@ void build_photon_tree(const float* pos, const float* nrm, const float* power, s
     out->nrm4[4 * i + 3] = 0.f;
     out->pow4[4 * i + 3] = 0.f;
   }
+  // 32-ary box levels over the kd leaves (the leaves are the heap's last
+  // level, left to right = leaf order)
+  const size_t nleaf = (size_t)1 << depth;
+  const size_t first = nleaf - 1;
+  out->leaf.resize(2 * nleaf);
+  std::vector<float> lo(3 * nleaf), hi(3 * nleaf);
+  for (size_t j = 0; j < nleaf; ++j) {
+    const PNode& nd = out->nodes[first + j];
+    out->leaf[2 * j] = nd.begin;
+    out->leaf[2 * j + 1] = nd.end;
+    for (int a = 0; a < 3; ++a) {
+      lo[3 * j + a] = INFINITY;
+      hi[3 * j + a] = -INFINITY;
+    }
+    for (uint32_t i = nd.begin; i < nd.end; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[3 * j + a] = std::min(lo[3 * j + a], out->pos4[4 * (size_t)i + a]);
+        hi[3 * j + a] = std::max(hi[3 * j + a], out->pos4[4 * (size_t)i + a]);
+      }
+  }
+  size_t count = nleaf;
+  int lvl = 0;
+  for (;;) {
+    if (lvl >= kPhotonMaxLevels) throw std::runtime_error("photon box tree too deep");
+    const size_t pad = (count + 31) / 32 * 32;
+    out->lvl_count[lvl] = (uint32_t)count;
+    out->lvl_pad[lvl] = (uint32_t)pad;
+    out->lvl_off[lvl] = (uint32_t)out->box.size();
+    const size_t o = out->box.size();
+    out->box.resize(o + 6 * pad);
+    for (size_t j = 0; j < pad; ++j)
+      for (int a = 0; a < 3; ++a) {
+        out->box[o + a * pad + j] = j < count ? lo[3 * j + a] : INFINITY;
+        out->box[o + (3 + a) * pad + j] = j < count ? hi[3 * j + a] : -INFINITY;
+      }
+    ++lvl;
+    if (count <= 32) break;
+    const size_t up = (count + 31) / 32;
+    std::vector<float> ulo(3 * up, INFINITY), uhi(3 * up, -INFINITY);
+    for (size_t j = 0; j < count; ++j)
+      for (int a = 0; a < 3; ++a) {
+        ulo[3 * (j / 32) + a] = std::min(ulo[3 * (j / 32) + a], lo[3 * j + a]);
+        uhi[3 * (j / 32) + a] = std::max(uhi[3 * (j / 32) + a], hi[3 * j + a]);
+      }
+    lo.swap(ulo);
+    hi.swap(uhi);
+    count = up;
+  }
+  out->nlevels = lvl;
+  if (out->box.size() > 0xffffffffu) throw std::runtime_error("photon box tree too large");
 }
 
 }  // namespace enc

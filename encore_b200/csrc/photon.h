@@ -23,19 +23,41 @@ struct PNode {
   uint32_t end;
 };
 
+// The gather walks a 32-ary box tree over the kd leaves, so that one warp
+// step tests 32 children (one per lane) instead of one binary split:
+//   level 0 = the kd leaves in leaf order (photon ranges, at most 32 each);
+//   level l = groups of 32 consecutive level-(l-1) items (a kd subtree five
+//             levels deep), item j covering items 32j .. 32j+31 below;
+//   the top level has at most 32 items and is the root's children.
+// Each level stores its items' boxes (the photons' bounds) as six float
+// arrays lo.x, lo.y, lo.z, hi.x, hi.y, hi.z of `pad` entries (count rounded
+// up to 32, padding boxes inverted so nothing enters them).
+constexpr int kPhotonMaxLevels = 8;
+
 struct PhotonHost {
   std::vector<PNode> nodes;   // heap order: children of i at 2i+1, 2i+2
   std::vector<float> pos4;    // x, y, z, original index (int bits)
   std::vector<float> nrm4;    // nx, ny, nz, 0
   std::vector<float> pow4;    // r, g, b, 0
   int depth = 0;
+  std::vector<uint32_t> leaf;  // (begin, end) per level-0 item
+  std::vector<float> box;      // all levels' box arrays, level 0 first
+  int nlevels = 0;
+  uint32_t lvl_count[kPhotonMaxLevels] = {};
+  uint32_t lvl_off[kPhotonMaxLevels] = {};  // float offset of the level in `box`
+  uint32_t lvl_pad[kPhotonMaxLevels] = {};
 };
 
 void build_photon_tree(const float* pos, const float* nrm, const float* power, size_t n,
                        PhotonHost* out);
 
 struct DevPhotonMap {
-  PNode* d_nodes = nullptr;
+  float* d_box = nullptr;      // PhotonHost::box
+  uint32_t* d_leaf = nullptr;  // PhotonHost::leaf
+  int nlevels = 0;
+  uint32_t lvl_count[kPhotonMaxLevels] = {};
+  uint32_t lvl_off[kPhotonMaxLevels] = {};
+  uint32_t lvl_pad[kPhotonMaxLevels] = {};
   float* d_pos4 = nullptr;
   float* d_nrm4 = nullptr;
   float* d_pow4 = nullptr;

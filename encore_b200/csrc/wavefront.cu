@@ -364,18 +364,30 @@ enc_status enc_photons_trace_device(enc_accel accel, const enc_photon_opts* o, f
   P.emit_offset = o->emit_offset;
   P.bounce_offset = o->bounce_offset;
   const size_t n = o->nphotons;
-  float* rays[2] = {nullptr, nullptr};
-  uint32_t* path[2] = {nullptr, nullptr};
-  int4* hits = nullptr;
-  uint32_t* counters = nullptr;
+  WaveScratch& w = *accel_wave_scratch(accel);
+  std::lock_guard<std::mutex> lk(w.mu);
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
-    e = cudaMalloc((void**)&rays[i], n * 32);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&path[i], n * 4);
+  if (w.cap < n) {  // grow the kept scratch (no allocation once it is large enough)
+    free_wave_scratch(&w);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+      e = cudaMalloc((void**)&w.rays[i], n * 32);
+      if (e == cudaSuccess) e = cudaMalloc((void**)&w.path[i], n * 4);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&w.hits, n * 16);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&w.counters, 16);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&w.h_counts, 16);
+    if (e != cudaSuccess) {
+      free_wave_scratch(&w);
+      set_error(std::string("enc_photons_trace_device: ") + cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? ENC_ERR_OUT_OF_MEMORY : ENC_ERR_CUDA;
+    }
+    w.cap = n;
   }
-  if (e == cudaSuccess) e = cudaMalloc((void**)&hits, n * 16);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&counters, 16);
-  if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 16, s);
+  float* const* rays = w.rays;
+  uint32_t* const* path = w.path;
+  int4* hits = static_cast<int4*>(w.hits);
+  uint32_t* counters = w.counters;
+  e = cudaMemsetAsync(counters, 0, 16, s);
   Launch L = resolve_launch(nullptr, a->kind, a->width);
   uint32_t count = o->nphotons;
   int cur = 0;
@@ -395,19 +407,15 @@ enc_status enc_photons_trace_device(enc_accel accel, const enc_photon_opts* o, f
         P, tri_view(*a), wave, hits, path[cur], count, d_pos, d_nrm, d_pow, capacity, counters,
         rays[cur ^ 1], path[cur ^ 1]);
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&count, counters + 1, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_counts, counters, 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    count = w.h_counts[1];
     cur ^= 1;
   }
   uint32_t total = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, counters, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_counts, counters, 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  for (int i = 0; i < 2; ++i) {
-    cudaFree(rays[i]);
-    cudaFree(path[i]);
-  }
-  cudaFree(hits);
-  cudaFree(counters);
+  if (e == cudaSuccess) total = w.h_counts[0];
   if (e != cudaSuccess) {
     set_error(std::string("enc_photons_trace_device: ") + cudaGetErrorString(e));
     return ENC_ERR_CUDA;
