@@ -32,6 +32,7 @@ def port():
         lib = C.CDLL(str(PORT_SO))
         lib.eo_tri_test.argtypes = [P, P, C.c_int, P, P, P]
         lib.eo_tri_test.restype = C.c_int
+        lib.eo_tri_test_batch.argtypes = [P, P, P, C.c_long, C.c_int, P, P, P, P]
         lib.eo_closest_brute.argtypes = [P, C.c_int, P, C.c_long, C.c_int, P, C.c_int]
         lib.eo_occluded_brute.argtypes = [P, C.c_int, P, C.c_long, C.c_int, P, C.c_int]
         lib.eo_closest_f64.argtypes = [P, C.c_int, P, C.c_long, P, C.c_int]
@@ -122,18 +123,14 @@ def tri_test(tris, rays, ids, clamp=True):
     """The FP32 reference predicate for ray i against triangle ids[i]:
     (accepted, t, alpha, beta)."""
     lib = port()
-    acc = np.zeros(len(ids), bool)
-    out = np.zeros((len(ids), 3), np.float32)
-    t, a, b = C.c_float(), C.c_float(), C.c_float()
-    tris = _c(tris)
-    rays = _c(rays)
-    for i, k in enumerate(np.asarray(ids)):
-        if k < 0:
-            continue
-        acc[i] = bool(lib.eo_tri_test(tris[k].ctypes.data, rays[i].ctypes.data, int(clamp),
-                                      C.byref(t), C.byref(a), C.byref(b)))
-        out[i] = (t.value, a.value, b.value)
-    return acc, out[:, 0], out[:, 1], out[:, 2]
+    tris, rays = _c(tris), _c(rays)
+    ids = _c(np.asarray(ids, dtype=np.int32))
+    n = len(ids)
+    acc = np.zeros(n, np.uint8)
+    t, a, b = (np.zeros(n, np.float32) for _ in range(3))
+    lib.eo_tri_test_batch(tris.ctypes.data, rays.ctypes.data, ids.ctypes.data, n, int(clamp),
+                          acc.ctypes.data, t.ctypes.data, a.ctypes.data, b.ctypes.data)
+    return acc.astype(bool), t, a, b
 
 
 def classify(tris, rays, got, want):

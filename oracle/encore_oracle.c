@@ -105,6 +105,18 @@ int eo_tri_test(const float* tri, const float* r, int clamp, float* t, float* al
   return (a >= 0.0) && (b >= 0.0) && (a + b <= 1) && (time > r[3]);
 }
 
+/* eo_tri_test for ray i against triangle ids[i] (ids[i] < 0: not tested). */
+void eo_tri_test_batch(const float* tris, const float* rays, const int* ids, long n, int clamp,
+                       uint8_t* acc, float* t, float* alpha, float* beta) {
+  for (long i = 0; i < n; ++i) {
+    acc[i] = 0;
+    t[i] = alpha[i] = beta[i] = 0.f;
+    if (ids[i] < 0) continue;
+    acc[i] = (uint8_t)eo_tri_test(tris + 9 * (size_t)ids[i], rays + 8 * (size_t)i, clamp, t + i,
+                                  alpha + i, beta + i);
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 /* brute force                                                               */
 

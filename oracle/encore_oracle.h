@@ -32,6 +32,9 @@ typedef struct eo_hit {
  * ClampfloatoZero to the Cross() results (Vector3.h:148-161). */
 int eo_tri_test(const float* tri9, const float* ray8, int clamp, float* t, float* alpha,
                 float* beta);
+/* eo_tri_test for ray i against triangle ids[i] (ids[i] < 0: not tested). */
+void eo_tri_test_batch(const float* tris, const float* rays, const int* ids, long n, int clamp,
+                       uint8_t* acc, float* t, float* alpha, float* beta);
 
 /* Brute-force closest hit over all triangles in ID order, strict-less
  * replacement (BasicAS::intersect, BasicAS.cpp:167-194). */
