@@ -166,6 +166,9 @@ struct Launch {
   int blocks_per_sm = 4;
   int chunk = 32;
   int stack = 32;
+  // Closest hit with one triangle loop per lane instead of the warp-wide
+  // triangle rounds: the host-buffer pipeline uses it (see host_form).
+  bool per_lane = false;
 };
 Launch resolve_launch(const enc_launch_opts* o, int kind, int width);
 

@@ -29,17 +29,16 @@
 
 #include "engine.h"
 
-// Build-time tuning of the wide-BVH kernel:
-//   ENC_TRACE_MINBLOCKS resident 128-thread blocks per SM the register
-//                       budget is fitted to.  The kernel waits on dependent
-//                       node loads, so resident warps pay: 10 (48 registers,
-//                       a few bytes spilled, width-8 stack entries of 8
-//                       bytes) ran 3.6 % faster than 8 (64 registers) on the
-//                       2M-triangle heightfield workload; 12 (40 registers)
-//                       spilled enough to lose 11 %.
-#ifndef ENC_TRACE_MINBLOCKS
-#define ENC_TRACE_MINBLOCKS 10
-#endif
+// Resident 128-thread blocks per SM that each kernel's register budget is
+// fitted to (also the default grid: SMs x this).  The closest-hit kernel
+// tests triangles cooperatively across the warp (below), which needs 64
+// registers: at 8 blocks it ran 4.5 % faster than the per-lane loop at its
+// best (10 blocks, 48 registers) on the 2M-triangle heightfield workload,
+// while at 9 or 10 blocks its spills cost more than the extra warps gave.
+// The any-hit kernel keeps the per-lane loop (its rays rarely reach a
+// triangle before the first hit) and 10 blocks.
+constexpr int kBlocksClosest = 8;
+constexpr int kBlocksAny = 10;
 
 namespace enc {
 namespace {
@@ -97,6 +96,16 @@ __device__ __forceinline__ bool tri_test(const float4 a, const float4 b, const f
   beta = fm(dot3(dx, dy, dz, qx, qy, qz), invdet);
   t = fm(dot3(e2x, e2y, e2z, qx, qy, qz), invdet);
   return (alpha >= 0.0f) && (beta >= 0.0f) && (fa(alpha, beta) <= 1.0f) && (t > tmin);
+}
+
+// A float's bits made monotone as an unsigned integer (negative values
+// below positive ones, order kept within each sign), and back.
+__device__ __forceinline__ uint32_t order_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float from_order_key(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
 struct TraceParams {
@@ -173,8 +182,9 @@ __device__ __forceinline__ void sort_net<4>(float (&k)[4], uint32_t (&v)[4]) {
 }
 #undef ENC_CSWAP
 
-template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false>
-__global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TraceParams P) {
+template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false, bool LANE = false>
+__global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClosest)
+    wbvh_trace(TraceParams P) {
   using L = WNodeLayout<W>;
   // Stack of node groups: one entry per visited node that still has hit
   // internal children, so the depth never exceeds the tree depth.
@@ -192,6 +202,13 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
   //   memory and leaves more of the SM's L1 to node and triangle loads.
   constexpr bool kCompact = W == 8;
   extern __shared__ uint2 s_stack[];
+  // Closest hit tests the triangles of the lanes' hit leaves as one warp
+  // (see below); any hit, and closest hit with LANE, keep one loop per lane.
+  constexpr bool kCoop = !ANY && !LANE;
+  __shared__ uint32_t s_coop_tri[kCoop ? 128 : 1];
+  __shared__ uint32_t s_coop_own[kCoop ? 128 : 1];
+  __shared__ unsigned long long s_coop_key[kCoop ? 128 : 1];
+  __shared__ float2 s_coop_uv[kCoop ? 128 : 1];
   const int B = blockDim.x;
   uint2* stk = s_stack + threadIdx.x;  // entry i at stk[i * B]
   float* slb = reinterpret_cast<float*>(s_stack + (size_t)P.stack_depth * B) + threadIdx.x;
@@ -291,9 +308,10 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
     }
     if (__all_sync(kFull, ray < 0)) break;
 
+    bool done = false;
+    bool hit_any = false;
+    uint32_t tmask = 0, tbase = 0;  // triangles of the node's hit leaves
     if (ray >= 0) {
-      bool done = false;
-      bool hit_any = false;
       if (++steps > kMaxSteps) {
         atomicOr(P.status, kStatusWatchdog);
         best_id = -1;
@@ -466,6 +484,9 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
           }
         }
         // ---- triangles of the hit leaves ---------------------------------
+        tmask = trimask;
+        tbase = tri_base;
+        if (kCoop) trimask = 0;  // tested below by the whole warp
         while (trimask) {
           const uint32_t k = __ffs(trimask) - 1;
           trimask &= trimask - 1;
@@ -495,6 +516,108 @@ __global__ void __launch_bounds__(128, ENC_TRACE_MINBLOCKS) wbvh_trace(TracePara
         }
         if (ANY && hit_any) done = true;
       }
+    }
+    if constexpr (kCoop) {
+    // ---- the warp tests all lanes' pending triangles together -------------
+    // Each round lists up to 32 (lane, triangle) items in shared memory; lane
+    // w tests item w with the owner lane's ray, and the owner's closest hit
+    // is the minimum of (t, ID) over its accepted candidates, taken with a
+    // 64-bit shared atomicMin on an order-preserving key (t's bits made
+    // monotone, then the ID) -- the same choice as the per-lane loop's
+    // "t < best_t, or equal t and a lower ID", whatever the order.
+    {
+      unsigned pend = __ballot_sync(kFull, tmask != 0);
+      const unsigned wib = threadIdx.x >> 5;
+      uint32_t* it_tri = s_coop_tri + wib * 32;
+      uint32_t* it_own = s_coop_own + wib * 32;
+      unsigned long long* key = s_coop_key + wib * 32;
+      float2* uv = s_coop_uv + wib * 32;
+      while (pend) {
+        const int ni = __popc(tmask);
+        int incl = ni;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int t = __shfl_up_sync(kFull, incl, d);
+          if ((int)lane >= d) incl += t;
+        }
+        const int excl = incl - ni;
+        const int total = __shfl_sync(kFull, incl, 31);
+        int j = 0;
+        while (tmask && excl + j < 32) {
+          const uint32_t k = __ffs(tmask) - 1;
+          tmask &= tmask - 1;
+          it_tri[excl + j] = tbase + k;
+          it_own[excl + j] = lane;
+          ++j;
+        }
+        if (COUNT) ntest += j;
+        const unsigned long long mykey =
+            ((unsigned long long)order_key(best_t) << 32) | (uint32_t)best_id;
+        key[lane] = mykey;
+        __syncwarp();
+        const int nitems = total < 32 ? total : 32;
+        const int own = (int)lane < nitems ? (int)it_own[lane] : (int)lane;
+        const float wox = __shfl_sync(kFull, ox, own), woy = __shfl_sync(kFull, oy, own),
+                    woz = __shfl_sync(kFull, oz, own);
+        const float wdx = __shfl_sync(kFull, dx, own), wdy = __shfl_sync(kFull, dy, own),
+                    wdz = __shfl_sync(kFull, dz, own);
+        const float wtmin = __shfl_sync(kFull, tmin, own);
+        const float wlim = __shfl_sync(kFull, ANY ? tmax : best_t, own);
+        const int wbid = __shfl_sync(kFull, best_id, own);
+        const float4* wtris = l_tris;
+        unsigned wntris = l_ntris;
+        if constexpr (MULTI) {
+          const unsigned long long tp = __shfl_sync(kFull, (unsigned long long)l_tris, own);
+          wtris = reinterpret_cast<const float4*>(tp);
+          wntris = __shfl_sync(kFull, l_ntris, own);
+        }
+        bool cand = false;
+        unsigned long long ckey = 0;
+        float cu = 0.f, cv = 0.f;
+        if ((int)lane < nitems) {
+          const uint32_t ti = it_tri[lane];
+          if (ti >= wntris) {
+            atomicOr(P.status, kStatusBounds);
+          } else {
+            const float4* tp = wtris + 3 * (size_t)ti;
+            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t, u, v;
+            if (tri_test<CLAMP>(a, b, c, wox, woy, woz, wdx, wdy, wdz, wtmin, t, u, v)) {
+              const int id = __float_as_int(c.y);
+              if (ANY) {
+                if (t < wlim) key[own] = 0ull;  // any hit: the owner is done
+              } else if (t < wlim || (t == wlim && id < wbid)) {
+                cand = true;
+                ckey = ((unsigned long long)order_key(t) << 32) | (uint32_t)id;
+                cu = u;
+                cv = v;
+                atomicMin(&key[own], ckey);
+              }
+            }
+          }
+        }
+        __syncwarp();
+        if (cand && key[own] == ckey) uv[own] = make_float2(cu, cv);
+        __syncwarp();
+        const unsigned long long nk = key[lane];
+        if (ANY) {
+          if (nk == 0ull && ray >= 0) {
+            hit_any = true;
+            done = true;
+            tmask = 0;
+          }
+        } else if (nk != mykey) {
+          best_t = from_order_key((uint32_t)(nk >> 32));
+          best_id = (int)(uint32_t)nk;
+          bu = uv[lane].x;
+          bv = uv[lane].y;
+        }
+        __syncwarp();
+        pend = __ballot_sync(kFull, tmask != 0);
+      }
+    }
+    }
+    if (ray >= 0) {
       // ---- pop the next group child that can still matter ----------------
       if (!done && node == kNoItem) {
         while (sp > 0) {
@@ -730,14 +853,16 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
   p.stack_depth = L.stack > 0 ? L.stack : (a.tree_depth > 8 ? a.tree_depth : 8);
   p.chunk = L.chunk;
   size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
-  auto k = wbvh_trace<W, CLAMP, ANY, COUNT>;
+  const bool lane = !ANY && L.per_lane;
+  auto k = lane ? wbvh_trace<W, CLAMP, ANY, COUNT, false, true> : wbvh_trace<W, CLAMP, ANY, COUNT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
   }
   cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return (int)e;
-  int grid = device_sm_count(a.device) * L.blocks_per_sm;
+  int grid = device_sm_count(a.device) *
+             (L.blocks_per_sm > 0 ? L.blocks_per_sm : ((ANY || lane) ? kBlocksAny : kBlocksClosest));
   k<<<grid, L.block, smem, s>>>(p);
   return (int)cudaGetLastError();
 }
@@ -844,7 +969,7 @@ int launch_w_external(const DevAccel& a, const float* rays, size_t n, enc_hit* h
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
   }
-  int grid = device_sm_count(a.device) * L.blocks_per_sm;
+  int grid = device_sm_count(a.device) * (L.blocks_per_sm > 0 ? L.blocks_per_sm : kBlocksClosest);
   k<<<grid, L.block, smem, s>>>(p);
   return (int)cudaGetLastError();
 }
@@ -895,7 +1020,8 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   }
   cudaError_t e = cudaMemsetAsync(m.d_counter, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return (int)e;
-  int grid = device_sm_count(m.device) * L.blocks_per_sm;
+  int grid = device_sm_count(m.device) *
+             (L.blocks_per_sm > 0 ? L.blocks_per_sm : (ANY ? kBlocksAny : kBlocksClosest));
   k<<<grid, L.block, smem, s>>>(p);
   return (int)cudaGetLastError();
 }
