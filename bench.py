@@ -620,6 +620,25 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     got = d_hits.cpu().numpy()
     assert np.array_equal(got[:, 0], hits_ref["tri"]), "timed kernel output differs"
 
+    # the kd-tree parity mode (the reference Kdtree's own cells and order,
+    # bit-exact with it) on the same batch, for scale against the wide BVH
+    kd_value = None
+    if not args.no_extras:
+        t_kd = time.perf_counter()
+        kd = Accelerator("kdtree", device=dev).build(tris)
+        kd_build_s = time.perf_counter() - t_kd
+
+        def kd_closest():
+            kd.intersect_device(d_rays, n, d_hits, launch=None, stream=stream)
+
+        for _ in range(2):
+            kd_closest()
+        ms_kd = timed(kd_closest, max(1, args.steps // 4))
+        kd.check(stream)
+        kd_rate, _ = replicas.aggregate_rate(n, len(ms_kd), sum(ms_kd))
+        kd_value = {"mrays_s": round(kd_rate / 1e6, 3), "build_seconds": round(kd_build_s, 2)}
+        kd.destroy()
+
     # algorithmic bytes per ray from the engine's own traversal counts
     d_vis = torch.empty((n, 2), dtype=torch.int32, device=dev)
     acc.count_visits(d_rays, n, d_vis, stream=stream)
@@ -701,6 +720,7 @@ def run_engine_arm(args, rank: int, world: int) -> None:
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(rays.nbytes), "d2h_bytes_per_step": int(n * 16)},
             "anyhit_mrays_s": round(any_value, 3),
+            "kdtree_mode": kd_value,
             "build_seconds": round(info["build_seconds"], 3),
             "clocks": clk,
             "cpu_baseline": cpu,
