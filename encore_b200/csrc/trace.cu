@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
             if (tn <= tf) {
               hm |= 1u << c;
-              if ((imask >> c) & 1u) lbmin = fminf(lbmin, tn);
+              // (any hit never culls by distance, so it keeps no bound)
+              if (!ANY && ((imask >> c) & 1u)) lbmin = fminf(lbmin, tn);
             }
           }
           // triangles of the hit leaves (meta = count << 5 | offset)
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
                 done = true;
               } else {
                 if constexpr (kCompact) {
-                  const uint32_t lb16 = lbmin >= 0.0f ? (__float_as_uint(lbmin) >> 16) : 0xff80u;
+                  const uint32_t lb16 =
+                      ANY ? 0u : (lbmin >= 0.0f ? (__float_as_uint(lbmin) >> 16) : 0xff80u);
                   stk[sp * B] = make_uint2(child_base, rest | (imask << 8) | (lb16 << 16));
                 } else {
                   stk[sp * B] = make_uint2(child_base, rest | (imask << 8));
