@@ -292,9 +292,19 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         // exactly 0) gives finite slab distances instead of 0 * inf = NaN,
         // which would leave that axis unconstrained.  The triangle predicate
         // keeps the exact direction.
-        ix = 1.0f / (fabsf(dx) > 1e-20f ? dx : copysignf(1e-20f, dx));
-        iy = 1.0f / (fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy));
-        iz = 1.0f / (fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz));
+        // The hardware reciprocal (rcp.approx, within 1 ulp) is enough here:
+        // an error of an ulp scales one axis's slab distances by 1 +- 2^-23,
+        // far inside the 1e-5 padding that keeps every accepted hit point off
+        // its box's faces, and it saves an IEEE division per axis each time a
+        // lane takes a new ray (measured +2.4 % closest, +3 % any hit).
+        auto rcp = [](float x) {
+          float r;
+          asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+          return r;
+        };
+        ix = rcp(fabsf(dx) > 1e-20f ? dx : copysignf(1e-20f, dx));
+        iy = rcp(fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy));
+        iz = rcp(fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz));
         octm = (dx < 0.f ? 1u : 0u) | (dy < 0.f ? 2u : 0u) | (dz < 0.f ? 4u : 0u);
         best_t = tmax; best_id = -1; bu = 0.f; bv = 0.f;
         sp = 0;
