@@ -267,8 +267,19 @@ def c0_section(dev: int, args, flush) -> dict:
         ms.append(a.elapsed_time(b))
     acc.check(stream)
     rate = n * len(ms) / (sum(ms) * 1e-3) / 1e6
+    # algorithmic bytes per ray from the kernel's own counts, as for the main line
+    info = acc.info()
+    d_vis = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    acc.count_visits(d_rays, n, d_vis, stream=stream)
+    vis = d_vis.cpu().numpy().astype(np.int64)
+    bpr = 32 + 16 + vis[:, 0].mean() * info["node_bytes"] / max(1, info["nnodes"]) + vis[:, 1].mean() * 48
+    pk = ROOT / "MEASURED_PEAKS.json"
+    hbm = json.loads(pk.read_text()).get("hbm_gbs", 6650.0) if pk.exists() else 6650.0
+    achieved = bpr * rate * 1e6 / 1e9
     out = {"workload": "10k random triangles (unit cube), 1024x1024 primary rays, unit scale",
-           "mrays_s": round(rate, 1), "ms_per_step": round(sum(ms) / len(ms), 4)}
+           "mrays_s": round(rate, 1), "ms_per_step": round(sum(ms) / len(ms), 4),
+           "roofline": {"bytes_per_ray": round(float(bpr), 1), "achieved_gbs": round(achieved, 1),
+                        "frac": round(achieved / hbm, 4)}}
     if not args.no_cpu:
         sub = rays[np.random.default_rng(3).choice(n, 65536, replace=False)]
         crate, kind, cores, build_s, _ = cpu_reference_rate(tris, sub, steps=1, warmup=0)
