@@ -1,15 +1,18 @@
 // Ray traversal kernels for sm_100a.
 //
-//  * wbvh_trace<W, CLAMP, ANY, COUNT>: persistent warps over the quantised
-//    wide BVH.  Each warp takes rays from a global atomic queue in chunks and
-//    hands them to idle lanes as lanes finish (no lane waits for the slowest
-//    ray of a batch).  The traversal stack lives in shared memory, one column
-//    per thread.  A visited node tests its triangles of hit leaves at once and
-//    continues with its first hit internal child; the others stay on the
-//    stack as one group entry.  Width 8 orders children by octant (the
-//    builder places each child in the slot of its octant, so slot k ^ octm
-//    for k = 0..7 is roughly front to back for a ray with direction sign
-//    bits octm); widths 2 and 4 sort hit children by entry distance.
+//  * wbvh_trace<W, CLAMP, ANY, COUNT, MULTI, LANE>: persistent warps over the
+//    quantised wide BVH.  Each warp takes rays from a global atomic queue in
+//    chunks and hands them to idle lanes as lanes finish (no lane waits for
+//    the slowest ray of a batch).  The traversal stack lives in shared
+//    memory, one column per thread.  A visited node continues with its first
+//    hit internal child; the others stay on the stack as one group entry.
+//    The triangles of its hit leaves are tested in the same step: for closest
+//    hit by the whole warp together (all lanes' triangles, one per lane per
+//    round), for any hit and with LANE by each lane in turn.  Width 8 orders
+//    children by octant (the builder places each child in the slot of its
+//    octant, so slot k ^ octm for k = 0..7 is roughly front to back for a ray
+//    with direction sign bits octm); widths 2 and 4 sort hit children by
+//    entry distance.  MULTI launches trace many scenes' batches at once.
 //  * kd_trace<CLAMP>: the reference's kd-tree walk (Kdtree.cpp:682-784), one
 //    thread per ray, over the flattened kd layout.  Bit-exact parity mode.
 //
