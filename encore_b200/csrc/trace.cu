@@ -212,6 +212,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
   __shared__ uint32_t s_coop_own[kCoop ? 128 : 1];
   __shared__ unsigned long long s_coop_key[kCoop ? 128 : 1];
   __shared__ float2 s_coop_uv[kCoop ? 128 : 1];
+  __shared__ float4 s_ray[kCoop ? 256 : 1];  // each lane's ray, for the rounds' workers
   const int B = blockDim.x;
   uint2* stk = s_stack + threadIdx.x;  // entry i at stk[i * B]
   float* slb = reinterpret_cast<float*>(s_stack + (size_t)P.stack_depth * B) + threadIdx.x;
@@ -290,6 +291,10 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         const float4 r1 = __ldg(rp + 1);
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
+        if (kCoop) {
+          s_ray[2 * threadIdx.x] = r0;
+          s_ray[2 * threadIdx.x + 1] = r1;
+        }
         // Box tests use a reciprocal with |d| floored at 1e-20 so that a zero
         // direction component (the reference's Normalize clamps small ones to
         // exactly 0) gives finite slab distances instead of 0 * inf = NaN,
@@ -572,11 +577,11 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         __syncwarp();
         const int nitems = total < 32 ? total : 32;
         const int own = (int)lane < nitems ? (int)it_own[lane] : (int)lane;
-        const float wox = __shfl_sync(kFull, ox, own), woy = __shfl_sync(kFull, oy, own),
-                    woz = __shfl_sync(kFull, oz, own);
-        const float wdx = __shfl_sync(kFull, dx, own), wdy = __shfl_sync(kFull, dy, own),
-                    wdz = __shfl_sync(kFull, dz, own);
-        const float wtmin = __shfl_sync(kFull, tmin, own);
+        // the owner's ray, kept in shared memory since its refill (two
+        // 16-byte loads instead of seven shuffles; measured +1 %)
+        const float4 wr0 = s_ray[2 * (wib * 32 + own)], wr1 = s_ray[2 * (wib * 32 + own) + 1];
+        const float wox = wr0.x, woy = wr0.y, woz = wr0.z, wtmin = wr0.w;
+        const float wdx = wr1.x, wdy = wr1.y, wdz = wr1.z;
         const float wlim = __shfl_sync(kFull, ANY ? tmax : best_t, own);
         const int wbid = __shfl_sync(kFull, best_id, own);
         const float4* wtris = l_tris;
