@@ -405,24 +405,28 @@ def served_section(dev: int, args) -> dict:
         from encore_b200.accel import HIT_DTYPE
         return p[4].numpy().view(HIT_DTYPE).reshape(p[2]) if p[1] == CLOSEST else p[4].numpy()
 
-    # plain: the per-request host-buffer call, back to back
-    svc = []
-    for rep in range(2):
-        svc = []
+    # plain: the per-request host-buffer call, back to back; best of 3 passes
+    # over the pool (host scheduling jitter only ever adds time), as for the
+    # server below
+    svc = None
+    for rep in range(3):
+        cur = []
         for p in pool:
             t1 = time.perf_counter()
             if p[1] == CLOSEST:
                 accs[p[0]].intersect(p[3].numpy(), out=out_view(p))
             else:
                 accs[p[0]].occluded(p[3].numpy(), out=out_view(p))
-            svc.append(time.perf_counter() - t1)
+            cur.append(time.perf_counter() - t1)
+        if svc is None or sum(cur) < sum(svc):
+            svc = cur
     plain_rate = total / sum(svc) / 1e6
     plain_ref = [out_view(p).copy() for p in pool]
 
     srv = Server(device=dev, slots=args.server_slots, slot_rays=args.server_slot_rays)
     ids = [srv.add_scene(a) for a in accs]
     sat = []
-    for rep in range(2):
+    for rep in range(3):
         t1 = time.perf_counter()
         rids = [srv.submit(ids[p[0]], p[3].numpy(), p[1], out=out_view(p)) for p in pool]
         for rid in rids:
