@@ -67,6 +67,12 @@ __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 
+// Stack entries.  An inner-node entry is level << 28 | item (level 1..7);
+// a leaf entry is kLeafEntry | first photon, with the leaf's photon count
+// kept beside it, so a leaf step reads its photons without first loading
+// its range.
+constexpr uint32_t kLeafEntry = 0x80000000u;
+
 // Position of the r-th set bit of m (r counted from 0, r < popc(m)), by
 // halving: keep the low half while it holds more than r set bits.
 __device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
@@ -84,36 +90,36 @@ __device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
 }
 
 // Max over the slots marked valid (slot index s*32 + lane < limit) and its
-// slot index; -INF / -1 if none.
+// slot index, the highest slot among equal maxima; -INF / -1 if none.  The
+// held values are squared distances, non-negative floats whose bit patterns
+// order as unsigned integers, so two warp max reductions (redux.sync) find
+// the value and then its slot.
 template <int S>
 __device__ __forceinline__ void warp_max(const float (&dd)[S], int lane, int limit, float& v,
                                          int& loc) {
-  v = -INFINITY;
-  loc = -1;
+  uint32_t lv = 0;
+  int ls = -1;
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int slot = s * 32 + lane;
-    if (slot < limit && (dd[s] > v || (dd[s] == v && slot > loc))) {
-      v = dd[s];
-      loc = slot;
+    const uint32_t u = __float_as_uint(dd[s]);
+    if (slot < limit && (ls < 0 || u >= lv)) {
+      lv = u;
+      ls = slot;
     }
   }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const float ov = __shfl_xor_sync(kFull, v, off);
-    const int ol = __shfl_xor_sync(kFull, loc, off);
-    if (ov > v || (ov == v && ol > loc)) {
-      v = ov;
-      loc = ol;
-    }
-  }
+  const uint32_t mv = __reduce_max_sync(kFull, ls >= 0 ? lv : 0u);
+  const uint32_t l1 = __reduce_max_sync(kFull, (ls >= 0 && lv == mv) ? (uint32_t)(ls + 1) : 0u);
+  loc = (int)l1 - 1;
+  v = l1 == 0 ? -INFINITY : __uint_as_float(mv);
 }
 
 template <int S, bool NEAREST>
 __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
-  // stack entries: level << 28 | item index, and the entry's squared distance
+  // stack entries, their squared distances, and a leaf entry's photon count
   __shared__ uint32_t s_item[kWarpsPerBlock][kStack];
   __shared__ float s_pd[kWarpsPerBlock][kStack];
+  __shared__ uint8_t s_cnt[kWarpsPerBlock][kStack];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -143,6 +149,7 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
       if (lane == 0) {
         s_item[wib][0] = (uint32_t)P.nlevels << 28;
         s_pd[wib][0] = 0.f;
+        s_cnt[wib][0] = 0;
       }
       sp = 1;
     }
@@ -156,14 +163,16 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
       --sp;
       const float pd = s_pd[wib][sp];
       const uint32_t e = s_item[wib][sp];
-      __syncwarp();
-      if (!(pd < r2)) continue;  // nothing in it can be accepted any more
-      const int lv = (int)(e >> 28);
-      const uint32_t it = e & 0x0fffffffu;
-      if (lv > 0) {
+      const int c0 = s_cnt[wib][sp];
+      if (!(pd < r2)) {  // nothing in it can be accepted any more
+        __syncwarp();
+        continue;
+      }
+      if (!(e & kLeafEntry)) {
+        __syncwarp();
         // inner node: lane c tests child 32 * it + c of level lv - 1
-        const int cl = lv - 1;
-        const uint32_t child = 32u * it + (uint32_t)lane;
+        const int cl = (int)(e >> 28) - 1;
+        const uint32_t child = 32u * (e & 0x0fffffffu) + (uint32_t)lane;
         bool pass = false;
         float cd = 0.f;
         if (child < P.lvl_count[cl]) {
@@ -187,20 +196,41 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
         }
         if (pass) {
           const int at = sp + __popc(m & lt);
-          s_item[wib][at] = ((uint32_t)cl << 28) | child;
+          uint32_t item = ((uint32_t)cl << 28) | child;
+          uint32_t cnt = 0;
+          if (cl == 0) {  // a leaf: its photon range goes onto the stack
+            const uint2 rng = __ldg(P.leaf + child);
+            item = kLeafEntry | rng.x;
+            cnt = rng.y - rng.x;
+          }
+          s_item[wib][at] = item;
           s_pd[wib][at] = cd;
+          s_cnt[wib][at] = (uint8_t)cnt;
         }
         sp += n;
         __syncwarp();
         continue;
       }
-      // leaf: lane j tests photon begin + j
-      const uint2 rng = __ldg(P.leaf + it);
-      const unsigned pidx = rng.x + (unsigned)lane;
+      // leaf: lane j tests photon j of the leaf; when the entry below is a
+      // leaf too and both fit in the warp, lanes c0.. test its photons
+      uint32_t b1 = 0;
+      int c1 = 0;
+      if (sp > 0) {
+        const uint32_t e1 = s_item[wib][sp - 1];
+        const int n1 = s_cnt[wib][sp - 1];
+        if ((e1 & kLeafEntry) && c0 + n1 <= 32 && s_pd[wib][sp - 1] < r2) {
+          b1 = e1 & ~kLeafEntry;
+          c1 = n1;
+          --sp;
+        }
+      }
+      __syncwarp();
+      const unsigned pidx = lane < c0 ? (e & ~kLeafEntry) + (unsigned)lane
+                                      : b1 + (unsigned)(lane - c0);
       bool acc = false;
       float d2 = 0.f;
       int orig = -1;
-      if (pidx < rng.y) {
+      if (lane < c0 + c1) {
         const float4 p = __ldg(P.pos4 + pidx);
         const float x = fs(qx, p.x), y = fs(qy, p.y), z = fs(qz, p.z);
         d2 = fa(fa(fm(x, x), fm(y, y)), fm(z, z));
@@ -216,51 +246,45 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
         // fill free heap slots in one step: the accepted candidate of rank r
         // (r-th set bit of m) goes to slot count + r, which lives on lane
         // (count + r) % 32, register (count + r) / 32
-        const int nfill = min(__popc(m), k - count);
+        const int na = __popc(m);
+        const int nfill = min(na, k - count);
         const int r = (lane - count) & 31;
         const bool take = r < nfill;
         const int src = nth_set_bit(m, take ? r : 0);
         const float cd = __shfl_sync(kFull, d2, src);
         const int co = __shfl_sync(kFull, orig, src);
+        const int cs = __shfl_sync(kFull, (int)pidx, src);
         const int slot = count + r;
         if (take) {
 #pragma unroll
           for (int s = 0; s < S; ++s)
             if (s == (slot >> 5)) {
               dd[s] = cd;
-              ds[s] = (int)rng.x + src;
+              ds[s] = cs;
               dorig[s] = co;
             }
         }
         // the first nfill set bits are done
-        for (int i = 0; i < nfill; ++i) m &= m - 1;
+        if (nfill == na) {
+          m = 0;
+        } else {
+          for (int i = 0; i < nfill; ++i) m &= m - 1;
+        }
         count += nfill;
         if (count == k) {
           warp_max<S>(dd, lane, k, worst, worst_loc);
           r2 = worst;
         }
       }
+      // the heap is full (a fill step leaves candidates only then): each
+      // closer candidate replaces the maximum
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1;
         const float cd = __shfl_sync(kFull, d2, j);
         const int co = __shfl_sync(kFull, orig, j);
-        const int cs = (int)rng.x + j;
-        if (count < k) {
-          const int slot = count;
-#pragma unroll
-          for (int s = 0; s < S; ++s)
-            if (lane == (slot & 31) && s == (slot >> 5)) {
-              dd[s] = cd;
-              ds[s] = cs;
-              dorig[s] = co;
-            }
-          ++count;
-          if (count == k) {
-            warp_max<S>(dd, lane, k, worst, worst_loc);
-            r2 = worst;
-          }
-        } else if (cd < worst) {
+        const int cs = __shfl_sync(kFull, (int)pidx, j);
+        if (cd < worst) {
 #pragma unroll
           for (int s = 0; s < S; ++s)
             if (lane == (worst_loc & 31) && s == (worst_loc >> 5)) {
@@ -365,18 +389,23 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
   p.r2max = max_dist * max_dist;  // maxDistance*maxDistance in FP32 (PhotonMap.cpp:89)
   p.ignore_normal = (flags & ENC_GATHER_IGNORE_NORMAL) ? 1 : 0;
   p.caustic = m.caustic;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
-  unsigned need = (unsigned)((nq + kWarpsPerBlock - 1) / kWarpsPerBlock);
-  unsigned grid = (unsigned)sms * 8;
-  if (grid > need) grid = need;
   const int S = k <= 32 ? 1 : (k <= 64 ? 2 : (k <= 128 ? 4 : 8));
-  switch (S) {
-    case 1: gather_kernel<1, NEAREST><<<grid, 256, 0, s>>>(p); break;
-    case 2: gather_kernel<2, NEAREST><<<grid, 256, 0, s>>>(p); break;
-    case 4: gather_kernel<4, NEAREST><<<grid, 256, 0, s>>>(p); break;
-    default: gather_kernel<8, NEAREST><<<grid, 256, 0, s>>>(p); break;
-  }
+  void (*kern)(GatherParams) = S == 1   ? gather_kernel<1, NEAREST>
+                               : S == 2 ? gather_kernel<2, NEAREST>
+                               : S == 4 ? gather_kernel<4, NEAREST>
+                                        : gather_kernel<8, NEAREST>;
+  // One resident wave: the warps stride over the queries, so a grid larger
+  // than the SMs hold would run its last blocks as a partly filled second
+  // wave (the register count allows 5 blocks of 256 threads per SM).
+  int sms = 148, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+  if (e != cudaSuccess) return (int)e;
+  if (per_sm < 1) per_sm = 1;
+  const unsigned need = (unsigned)((nq + kWarpsPerBlock - 1) / kWarpsPerBlock);
+  unsigned grid = (unsigned)sms * (unsigned)per_sm;
+  if (grid > need) grid = need;
+  kern<<<grid, 256, 0, s>>>(p);
   return (int)cudaGetLastError();
 }
 

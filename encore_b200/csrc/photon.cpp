@@ -136,6 +136,9 @@ void build_photon_tree(const float* pos, const float* nrm, const float* power, s
     hi.swap(uhi);
     count = up;
   }
+  // The gather's stack keeps a level below its leaf-entry bit (bit 31), so
+  // at most 7; 2^31 photons in leaves of 16 or more make at most 6.
+  if (lvl > 7) throw std::runtime_error("photon box tree too deep");
   out->nlevels = lvl;
   if (out->box.size() > 0xffffffffu) throw std::runtime_error("photon box tree too large");
 }
