@@ -655,6 +655,7 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
     if (e == cudaSuccess) e = upload(&d.d_pow4, h.pow4.data(), h.pow4.size());
     if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
     if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, kGatherSlots * sizeof(uint32_t));
   } catch (const std::exception& ex) {
     set_error(std::string("enc_photonmap_create: ") + ex.what());
     e = cudaErrorMemoryAllocation;
@@ -666,6 +667,7 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
     cudaFree(d.d_nrm4);
     cudaFree(d.d_pow4);
     cudaFree(d.d_status);
+    cudaFree(d.d_counter);
     delete m;
     return cuda_fail(e, "enc_photonmap_create");
   }
@@ -701,6 +703,7 @@ enc_status enc_photonmap_destroy(enc_photonmap m) {
   cudaFree(m->dev.d_nrm4);
   cudaFree(m->dev.d_pow4);
   cudaFree(m->dev.d_status);
+  cudaFree(m->dev.d_counter);
   cudaFree(m->d_stage);
   delete m;
   return ENC_OK;

@@ -3,19 +3,20 @@
 // One warp per query point.  The warp walks the 32-ary box tree over the
 // photon kd leaves (photon.h) with a per-warp stack in shared memory: at an
 // inner node each lane tests one child box against the search sphere and the
-// children that can hold an accepted photon are pushed together; at a leaf
-// each lane tests one photon (32-photon leaves = one coalesced 16-byte load
-// per lane per array).  A box is pruned by its FP32 squared distance to the
-// query, formed with the photon test's own operations on the box's clamped
-// coordinates; rounding is monotone, so that distance never exceeds the
-// squared distance of a photon inside the box and pruning drops nothing the
-// photon test would accept.  The k best candidates are kept in a warp-distributed bounded
-// max-heap: S = ceil(k/32) register slots per lane, slot i on lane i % 32; the
-// maximum and its owner are found with a 5-step shuffle reduction, and an
-// accepted candidate replaces it.  The search radius is max_dist^2 until k
-// photons are held and the heap maximum afterwards, as in
-// PhotonMap::GetNearestNPhotons (PhotonMap.cpp:224-297), so the result is the
-// exact k-nearest set.
+// children that can hold an accepted photon are pushed together (a leaf as
+// its photon range); at a leaf each lane tests one photon, and two sibling
+// leaves share one step when their photons fit in the warp (one coalesced
+// 16-byte load per lane per array).  A box is pruned by its FP32 squared
+// distance to the query, formed with the photon test's own operations on the
+// box's clamped coordinates; rounding is monotone, so that distance never
+// exceeds the squared distance of a photon inside the box and pruning drops
+// nothing the photon test would accept.  The k best candidates are kept in a
+// warp-distributed bounded max-heap: S = ceil(k/32) register slots per lane,
+// slot i on lane i % 32; the maximum and its slot are found with two warp max
+// reductions (redux.sync), and an accepted candidate replaces it.  The search
+// radius is max_dist^2 until k photons are held and the heap maximum
+// afterwards, as in PhotonMap::GetNearestNPhotons (PhotonMap.cpp:224-297), so
+// the result is the exact k-nearest set.
 //
 // Acceptance is the reference's: FP32 dist^2 = (x*x + y*y) + z*z with separate
 // roundings, dist^2 < r^2, and the stored surface normal equal to the query
@@ -38,6 +39,8 @@ constexpr int kWarpsPerBlock = 8;
 // 32 entries per level suffice.
 constexpr int kStack = 32 * kPhotonMaxLevels;
 constexpr unsigned kMaxSteps = 1u << 24;
+// Queries a warp takes from the queue at a time.
+constexpr unsigned kQueryChunk = 4;
 
 struct GatherParams {
   const float* box;
@@ -56,6 +59,7 @@ struct GatherParams {
   float* d2;
   int32_t* count;
   uint32_t* status;
+  uint32_t* counter;  // this launch's query-queue head, zeroed before it
   unsigned nq;
   int k;
   float r2max;
@@ -123,9 +127,22 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  const unsigned total = gridDim.x * kWarpsPerBlock;
   const int k = P.k;
-  for (unsigned q = blockIdx.x * kWarpsPerBlock + wib; q < P.nq; q += total) {
+  // Each warp takes kQueryChunk queries at a time from the launch's queue
+  // head, so every warp stays busy until the queue is empty (a fixed share
+  // per warp left a fifth of the warp slots idle at the end).  The head
+  // overshoots nq by at most kQueryChunk per warp: nq < 2^31 keeps it below
+  // 2^32.
+  unsigned q = 0, qend = 0;
+  for (;;) {
+    if (q == qend) {
+      unsigned b = 0;
+      if (lane == 0) b = atomicAdd(P.counter, kQueryChunk);
+      b = __shfl_sync(kFull, b, 0);
+      if (b >= P.nq) break;
+      q = b;
+      qend = min(b + kQueryChunk, P.nq);
+    }
     const float qx = __ldg(P.qpos + 3 * (size_t)q), qy = __ldg(P.qpos + 3 * (size_t)q + 1),
                 qz = __ldg(P.qpos + 3 * (size_t)q + 2);
     const float nx = __ldg(P.qnrm + 3 * (size_t)q), ny = __ldg(P.qnrm + 3 * (size_t)q + 1),
@@ -357,6 +374,7 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
         P.rgb[3 * (size_t)q + 2] = B;
       }
     }
+    ++q;
   }
 }
 
@@ -384,6 +402,9 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
   p.d2 = d2;
   p.count = count;
   p.status = m.d_status;
+  const uint32_t slot = __atomic_fetch_add(const_cast<uint32_t*>(&m.counter_seq), 1u,
+                                           __ATOMIC_RELAXED) % kGatherSlots;
+  p.counter = m.d_counter + slot;
   p.nq = (unsigned)nq;
   p.k = m.n == 0 ? 0 : k;
   p.r2max = max_dist * max_dist;  // maxDistance*maxDistance in FP32 (PhotonMap.cpp:89)
@@ -394,12 +415,14 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
                                : S == 2 ? gather_kernel<2, NEAREST>
                                : S == 4 ? gather_kernel<4, NEAREST>
                                         : gather_kernel<8, NEAREST>;
-  // One resident wave: the warps stride over the queries, so a grid larger
-  // than the SMs hold would run its last blocks as a partly filled second
-  // wave (the register count allows 5 blocks of 256 threads per SM).
+  // One resident wave of persistent warps (the register count allows 5
+  // blocks of 256 threads per SM): a larger grid would only queue blocks
+  // that find the query queue empty.
   int sms = 148, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemsetAsync(p.counter, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return (int)e;
   if (per_sm < 1) per_sm = 1;
   const unsigned need = (unsigned)((nq + kWarpsPerBlock - 1) / kWarpsPerBlock);

@@ -51,6 +51,8 @@ struct PhotonHost {
 void build_photon_tree(const float* pos, const float* nrm, const float* power, size_t n,
                        PhotonHost* out);
 
+constexpr int kGatherSlots = 256;
+
 struct DevPhotonMap {
   float* d_box = nullptr;      // PhotonHost::box
   uint32_t* d_leaf = nullptr;  // PhotonHost::leaf
@@ -62,6 +64,10 @@ struct DevPhotonMap {
   float* d_nrm4 = nullptr;
   float* d_pow4 = nullptr;
   uint32_t* d_status = nullptr;
+  // Query-queue heads: each launch takes the next of kGatherSlots words and
+  // zeroes it on its stream, so launches on different streams never share one.
+  uint32_t* d_counter = nullptr;
+  uint32_t counter_seq = 0;
   uint32_t nnodes = 0;
   uint32_t n = 0;
   int depth = 0;
