@@ -58,6 +58,31 @@ def test_gather_k_sweep_matches_fp64_oracle(gpu, k):
         assert np.array_equal(gcnt, cnt)
 
 
+@pytest.mark.parametrize("n", [65537, 67584])
+@pytest.mark.parametrize("k", [1, 50, 100])
+def test_gather_paired_leaves_match_fp64_oracle(gpu, n, k):
+    # The build splits down to leaves of at most 32 photons, so leaves hold
+    # between 16 and 32. Only just above 16 * 2^d do leaves of 16 appear,
+    # two of which the gather tests in one warp step. 65,537 photons give
+    # 4,096 leaves of 16 (one of 17); 67,584 give 16s and 17s half and half,
+    # so some sibling pairs fit in a step and some do not.
+    rng = np.random.default_rng(n + k)
+    pos = rng.random((n, 3), dtype=np.float32)
+    nrm = np.tile(np.array([[0, 1, 0]], np.float32), (n, 1))
+    nrm[::4] = (0, 0, 1)
+    pw = rng.random((n, 3), dtype=np.float32) / n
+    q = rng.random((2000, 3), dtype=np.float32)
+    qn = np.tile(np.array([[0, 1, 0]], np.float32), (2000, 1))
+    for caustic in (False, True):
+        pm = PhotonMap(n, caustic=caustic)
+        pm.add_photons(pos, nrm, pw)
+        rgb = pm.get_radiance_estimate(k, 0.06, q, qn)
+        want, cnt = ob.port_gather(pos, nrm, pw, q, qn, k, 0.06, caustic=caustic)
+        np.testing.assert_allclose(rgb, want, rtol=RTOL, atol=1e-12)
+        idx, d2, gcnt = pm.get_nearest_n_photons(k, 0.06, q, qn)
+        assert np.array_equal(gcnt, cnt)
+
+
 def test_gather_edge_cases(gpu):
     pm = PhotonMap(10)
     pm.balance_and_construct()  # empty map
