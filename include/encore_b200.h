@@ -382,7 +382,11 @@ enum {
 };
 
 /* GetRadianceEstimate (PhotonMap.cpp:121-164) for nq query points
- * (position + normal, 3 floats each); rgb gets 3 floats per query. */
+ * (position + normal, 3 floats each); rgb gets 3 floats per query.
+ * nq < 2^31 and k <= 256 (ENC_ERR_INVALID_ARG / ENC_ERR_UNSUPPORTED beyond).
+ * The _device form is asynchronous on `stream`.  Calls on one map from
+ * different streams may run at once: each launch takes its own work-queue
+ * head, one of 256 per map, in turn. */
 enc_status enc_photonmap_radiance(enc_photonmap map, const float* qpos, const float* qnrm,
                                   size_t nq, int32_t k, float max_dist, int32_t flags,
                                   float* rgb, enc_stream stream);
