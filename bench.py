@@ -54,23 +54,23 @@ def log(*a):
 # ---------------------------------------------------------------------------
 # inputs
 
-def make_scene(seed: int) -> np.ndarray:
+def make_scene(seed: int, scale: float = SCALE) -> np.ndarray:
     from encore_b200 import scenes
-    return scenes.heightfield(res=RES, seed=seed, scale=SCALE)
+    return scenes.heightfield(res=RES, seed=seed, scale=scale)
 
 
-def primary_rays(res: int) -> np.ndarray:
+def primary_rays(res: int, scale: float = SCALE) -> np.ndarray:
     from encore_b200 import scenes
-    return scenes.camera_rays(res, res, eye=np.array([0.5, 1.3, 0.5]) * SCALE,
-                              look=np.array([0.5, 0.0, 0.5]) * SCALE, up=(0.0, 0.0, 1.0),
+    return scenes.camera_rays(res, res, eye=np.array([0.5, 1.3, 0.5]) * scale,
+                              look=np.array([0.5, 0.0, 0.5]) * scale, up=(0.0, 0.0, 1.0),
                               fov_deg=40.0)
 
 
-def mixed_batch(tris, prim, hits, seed: int) -> np.ndarray:
+def mixed_batch(tris, prim, hits, seed: int, scale: float = SCALE) -> np.ndarray:
     """Primaries + 3 diffuse secondaries per primary hit, shuffled."""
     from encore_b200 import scenes
     sec = scenes.diffuse_rays(tris, prim, hits["tri"], hits["u"], hits["v"], per_hit=3,
-                              seed=seed, offset=1e-4 * SCALE)
+                              seed=seed, offset=1e-4 * scale)
     rays = np.concatenate([prim, sec])
     perm = np.random.default_rng(seed + 1).permutation(len(rays))
     return np.ascontiguousarray(rays[perm])

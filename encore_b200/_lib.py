@@ -51,6 +51,10 @@ class LaunchOpts(C.Structure):
                 ("stack_depth", C.c_int32)]
 
 
+class BinOpts(C.Structure):
+    _fields_ = [("origin_bits", C.c_int32), ("dir_bits", C.c_int32), ("probe_frac", C.c_float)]
+
+
 class AccelInfo(C.Structure):
     _fields_ = [("kind", C.c_int32), ("width", C.c_int32), ("predicate", C.c_int32),
                 ("ntris", C.c_uint32), ("nnodes", C.c_uint32), ("node_bytes", C.c_uint64),
@@ -84,6 +88,11 @@ class PhotonOpts(C.Structure):
     _fields_ = [("light_center", C.c_float * 3), ("light_size", C.c_float),
                 ("nphotons", C.c_uint32), ("max_bounces", C.c_uint32), ("albedo", C.c_float),
                 ("seed", C.c_uint32), ("emit_offset", C.c_float), ("bounce_offset", C.c_float)]
+
+
+class PhotonStore(C.Structure):
+    _fields_ = [("d_pos", C.c_void_p), ("d_nrm", C.c_void_p), ("d_pow", C.c_void_p),
+                ("d_tag", C.c_void_p), ("capacity", C.c_uint32)]
 
 
 class ModelXform(C.Structure):
@@ -132,6 +141,11 @@ SIGNATURES = {
     "enc_accel_info_get": (C.c_int32, [P, C.POINTER(AccelInfo)]),
     "enc_intersect_closest": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_bin_scratch_bytes": (C.c_int32, [C.c_size_t, C.POINTER(BinOpts),
+                                          C.POINTER(C.c_size_t)]),
+    "enc_intersect_closest_device_binned": (C.c_int32, [P, P, C.c_size_t, P, P, C.c_size_t,
+                                                        C.POINTER(BinOpts),
+                                                        C.POINTER(LaunchOpts), P]),
     "enc_intersect_any": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_intersect_any_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_accel_check": (C.c_int32, [P, P]),
@@ -157,12 +171,18 @@ SIGNATURES = {
                                             C.c_float, P, P]),
     "enc_photons_trace_device": (C.c_int32, [P, C.POINTER(PhotonOpts), P, P, P, C.c_uint32,
                                              C.POINTER(C.c_uint32), P]),
+    "enc_photons_trace_maps_device": (C.c_int32, [P, C.POINTER(PhotonOpts), C.c_float, C.c_int32,
+                                                  C.POINTER(PhotonStore), C.POINTER(PhotonStore),
+                                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P]),
     "enc_photonmap_create_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32,
                                                 C.POINTER(P)]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
+    "enc_photonmap_check": (C.c_int32, [P, P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),
     "enc_photonmap_radiance_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),
+    "enc_photonmap_count_visits": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float,
+                                               C.c_int32, P, P, P]),
     "enc_photonmap_nearest": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P, P, P]),
 }
 

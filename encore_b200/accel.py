@@ -30,6 +30,20 @@ PRED = {"reference": _lib.ENC_PRED_REFERENCE, "noclamp": _lib.ENC_PRED_NOCLAMP}
 
 
 @dataclass
+class BinConfig:
+    """Ray binning ahead of the closest-hit launch (enc_bin_opts): key bits of
+    the origin cell and of the direction cell (both 0 = the tuned default),
+    and the probe distance as a fraction of the scene diagonal (0 = bin the
+    origin itself)."""
+    origin_bits: int = 0
+    dir_bits: int = 0
+    probe_frac: float = 0.0
+
+    def c(self) -> _lib.BinOpts:
+        return _lib.BinOpts(self.origin_bits, self.dir_bits, self.probe_frac)
+
+
+@dataclass
 class LaunchConfig:
     block_threads: int = 0
     blocks_per_sm: int = 0
@@ -136,6 +150,28 @@ class Accelerator:
         check(self.lib.enc_intersect_closest_device(self.handle, ptr(d_rays), n, ptr(d_hits),
                                                     C.byref(lo), _stream_ptr(stream)),
               "enc_intersect_closest_device")
+
+    def bin_scratch_bytes(self, n: int, binning: BinConfig | None = None) -> int:
+        out = C.c_size_t()
+        b = (binning or BinConfig()).c()
+        check(self.lib.enc_bin_scratch_bytes(n, C.byref(b), C.byref(out)),
+              "enc_bin_scratch_bytes")
+        return out.value
+
+    def intersect_device_binned(self, d_rays, n: int, d_hits, d_scratch,
+                                binning: BinConfig | None = None,
+                                launch: LaunchConfig | None = None, stream=None) -> None:
+        """Closest hit with the batch binned first (identical hits); d_scratch
+        is a device buffer of at least bin_scratch_bytes(n) bytes (a torch
+        uint8 CUDA tensor, whose storage the caching allocator aligns to 512
+        bytes)."""
+        lo = (launch or LaunchConfig()).c()
+        b = (binning or BinConfig()).c()
+        nbytes = d_scratch.numel() * d_scratch.element_size() if hasattr(d_scratch, "numel") \
+            else int(getattr(d_scratch, "nbytes", 0))
+        check(self.lib.enc_intersect_closest_device_binned(
+            self.handle, ptr(d_rays), n, ptr(d_hits), ptr(d_scratch), nbytes, C.byref(b),
+            C.byref(lo), _stream_ptr(stream)), "enc_intersect_closest_device_binned")
 
     def occluded_device(self, d_rays, n: int, d_occ, launch: LaunchConfig | None = None,
                         stream=None) -> None:

@@ -135,8 +135,12 @@ void free_wave_scratch(WaveScratch* w) {
   for (int i = 0; i < 2; ++i) {
     cudaFree(w->rays[i]);
     cudaFree(w->path[i]);
+    cudaFree(w->srays[i]);
+    cudaFree(w->spath[i]);
     w->rays[i] = nullptr;
     w->path[i] = nullptr;
+    w->srays[i] = nullptr;
+    w->spath[i] = nullptr;
   }
   cudaFree(w->hits);
   cudaFree(w->counters);
@@ -322,6 +326,15 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
   }
   d.device_bytes = d.node_bytes + d.tri_bytes + (d.d_tri_pos ? 4ull * d.ntris : 0) +
                    kQueueSlots * sizeof(uint32_t) + 16;
+  // The no-allocation query entry point's fixed scratch on this device: its
+  // address is looked up now, while allocating is allowed (the look-up makes
+  // the runtime create the array).
+  const int pe = noalloc_prepare(d);
+  if (pe != 0) {
+    free_dev(d);
+    delete a;
+    return cuda_fail((cudaError_t)pe, "enc_accel_build: fixed query scratch");
+  }
   d.build_seconds = now_s() - t0;
   *out = a;
   return ENC_OK;
@@ -447,6 +460,89 @@ enc_status enc_intersect_closest_device(enc_accel a, const float* d_rays, size_t
     return ENC_ERR_INVALID_ARG;
   }
   int e = launch_closest(a->dev, d_rays, nrays, d_hits, L, stream, nullptr);
+  if (e != 0) return cuda_fail((cudaError_t)e, "closest-hit launch");
+  return ENC_OK;
+}
+
+namespace {
+
+// Default key: 16 bits, 10 of the origin cell and 6 of the direction.
+constexpr int kBinOriginBits = 10;
+constexpr int kBinDirBits = 6;
+
+bool resolve_bin(const enc_bin_opts* o, int* ob, int* db, float* probe) {
+  *ob = kBinOriginBits;
+  *db = kBinDirBits;
+  *probe = 0.0f;
+  if (o) {
+    if (o->origin_bits < 0 || o->dir_bits < 0 || !(o->probe_frac >= 0.0f) ||
+        o->probe_frac > 16.0f)
+      return false;
+    if (o->origin_bits != 0 || o->dir_bits != 0) {
+      *ob = o->origin_bits;
+      *db = o->dir_bits;
+    }
+    *probe = o->probe_frac;
+  }
+  return *ob + *db >= 1 && *ob + *db <= kBinMaxKeyBits && *db <= 2 * kBinMaxDimBits &&
+         *ob <= 3 * kBinMaxDimBits;
+}
+
+}  // namespace
+
+enc_status enc_bin_scratch_bytes(size_t nrays, const enc_bin_opts* bin, size_t* bytes) {
+  if (!bytes) return ENC_ERR_INVALID_ARG;
+  int ob, db;
+  float pf;
+  if (!resolve_bin(bin, &ob, &db, &pf)) {
+    set_error("enc_bin_scratch_bytes: origin_bits + dir_bits must be 1..20");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *bytes = bin_scratch_bytes(nrays, ob + db);
+  return ENC_OK;
+}
+
+enc_status enc_intersect_closest_device_binned(enc_accel a, const float* d_rays, size_t nrays,
+                                               enc_hit* d_hits, void* d_scratch,
+                                               size_t scratch_bytes, const enc_bin_opts* bin,
+                                               const enc_launch_opts* launch,
+                                               enc_stream stream) {
+  if (!a || (nrays && (!d_rays || !d_hits || !d_scratch))) {
+    set_error("enc_intersect_closest_device_binned: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays > 0xffffffffull / 2) {
+    set_error("enc_intersect_closest_device_binned: too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (a->dev.kind != ENC_ACCEL_WBVH) {
+    set_error("enc_intersect_closest_device_binned: wide BVH only");
+    return ENC_ERR_UNSUPPORTED;
+  }
+  int ob, db;
+  float pf;
+  if (!resolve_bin(bin, &ob, &db, &pf)) {
+    set_error("enc_intersect_closest_device_binned: origin_bits + dir_bits must be 1..20");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays == 0) return ENC_OK;
+  if (scratch_bytes < bin_scratch_bytes(nrays, ob + db) ||
+      (reinterpret_cast<uintptr_t>(d_scratch) & 255u) != 0) {
+    set_error("enc_intersect_closest_device_binned: scratch smaller than enc_bin_scratch_bytes "
+              "or not 256-byte aligned");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(a->dev.device);
+  Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 0 or 2..64)");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const BinSpec spec = make_bin_spec(a->dev.lo, a->dev.hi, ob + db, db, pf);
+  uint32_t* order = nullptr;
+  int e = launch_bin(d_rays, nrays, spec, d_scratch, &order, a->dev.device, stream);
+  if (e != 0) return cuda_fail((cudaError_t)e, "binning launch");
+  e = launch_closest(a->dev, d_rays, nrays, d_hits, L, stream, nullptr, order);
   if (e != 0) return cuda_fail((cudaError_t)e, "closest-hit launch");
   return ENC_OK;
 }
@@ -740,6 +836,12 @@ enc_status pmap_status(enc_photonmap m, cudaStream_t s) {
 }
 }  // namespace
 
+enc_status enc_photonmap_check(enc_photonmap m, enc_stream stream) {
+  if (!m) return ENC_ERR_INVALID_ARG;
+  DeviceScope ds(m->dev.device);
+  return pmap_status(m, static_cast<cudaStream_t>(stream));
+}
+
 enc_status enc_photonmap_radiance_device(enc_photonmap m, const float* d_qpos, const float* d_qnrm,
                                          size_t nq, int32_t k, float max_dist, int32_t flags,
                                          float* d_rgb, enc_stream stream) {
@@ -749,6 +851,19 @@ enc_status enc_photonmap_radiance_device(enc_photonmap m, const float* d_qpos, c
   int e = launch_radiance(m->dev, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, stream);
   if (e) return cuda_fail((cudaError_t)e, "gather launch");
   return ENC_OK;
+}
+
+enc_status enc_photonmap_count_visits(enc_photonmap m, const float* d_qpos, const float* d_qnrm,
+                                      size_t nq, int32_t k, float max_dist, int32_t flags,
+                                      float* d_rgb, uint32_t* d_visits, enc_stream stream) {
+  enc_status st = gather_args(m, nq, k, max_dist, d_qpos, d_qnrm, d_rgb, "enc_photonmap_count_visits");
+  if (st) return st;
+  if (nq && !d_visits) return ENC_ERR_INVALID_ARG;
+  DeviceScope ds(m->dev.device);
+  int e = launch_radiance_counted(m->dev, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, d_visits,
+                                  stream);
+  if (e) return cuda_fail((cudaError_t)e, "gather launch");
+  return pmap_status(m, static_cast<cudaStream_t>(stream));
 }
 
 enc_status enc_photonmap_radiance(enc_photonmap m, const float* qpos, const float* qnrm, size_t nq,

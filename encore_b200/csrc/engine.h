@@ -131,6 +131,9 @@ struct MultiLaunch {
   int stack_depth = 8;  // deepest scene's tree depth
   uint32_t* d_counter = nullptr;
   uint32_t* d_status = nullptr;
+  // optional: one status word per batch (a ray's loop-bound stop is recorded
+  // in its own batch's word instead of d_status)
+  uint32_t* d_batch_status = nullptr;
 };
 
 // Host results of the builders (before upload).
@@ -172,9 +175,35 @@ struct Launch {
 };
 Launch resolve_launch(const enc_launch_opts* o, int kind, int width);
 
-// Kernel launchers (trace.cu).  All asynchronous on `stream`.
+// ---------------------------------------------------------------------------
+// Ray binning (reorder.cu): a key per ray from its origin cell and direction
+// cell, counting-sorted into a permutation the traversal reads its queue
+// through.
+constexpr int kBinMaxDimBits = 10;  // bits per key dimension
+constexpr int kBinMaxKeyBits = 20;  // histogram of at most 2^20 buckets
+struct BinSpec {
+  float lo[3];     // low corner of the binned box
+  float scale[3];  // cells per unit length on each axis
+  float probe_len; // > 0: bin the point o + probe_len * d instead of o
+  int bits[5];     // key bits: origin x, y, z, direction u, v
+};
+// Scratch layout: keys (n words), order (n words), histogram (2^key_bits
+// words), each 256-byte aligned.
+size_t bin_scratch_bytes(size_t nrays, int key_bits);
+// key_bits total, dir_bits of them for the direction; the rest go to the
+// origin axes, widest cells first.  probe_frac: probe distance as a fraction
+// of the box diagonal (0 = the origin itself).
+BinSpec make_bin_spec(const float lo[3], const float hi[3], int key_bits, int dir_bits,
+                      float probe_frac);
+// Enqueues the three binning kernels on `s`; *d_order points into d_scratch.
+int launch_bin(const float* d_rays, size_t n, const BinSpec& spec, void* d_scratch,
+               uint32_t** d_order, int device, void* stream);
+
+// Kernel launchers (trace.cu).  All asynchronous on `stream`.  d_order (may
+// be null): queue index q traces ray d_order[q].
 int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_hits,
-                   const Launch& L, void* stream, uint32_t* d_visits);
+                   const Launch& L, void* stream, uint32_t* d_visits,
+                   const uint32_t* d_order = nullptr);
 int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
                const Launch& L, void* stream);
 // Wide-BVH closest hit whose queue head (*counter, zeroed by the caller on
@@ -182,6 +211,15 @@ int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ,
 int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size_t n,
                                     enc_hit* d_hits, const Launch& L, void* stream,
                                     uint32_t* counter, uint32_t* status);
+// Launches the closest-hit kernel of launch_closest_external_scratch for `a`
+// once over an empty batch and waits (trace.cu): its module is loaded and the
+// context's local memory sized for it, so a later launch allocates nothing.
+// `a.device` must be current; counter and status are device words.
+int warm_closest_kernel(const DevAccel& a, uint32_t* counter, uint32_t* status);
+// Resolves the no-allocation entry point's fixed scratch on `a.device` and
+// preloads its kernel (noalloc.cu); called by enc_accel_build, where
+// allocating is allowed.  `a.device` must be current.
+int noalloc_prepare(const DevAccel& a);
 // Closest hit for every batch of a multi-scene table in one persistent launch.
 int launch_multi_closest(const MultiLaunch& m, const Launch& L, void* stream);
 // Any hit (uint8 occluded per ray) for every batch of the table.
@@ -200,9 +238,12 @@ const DevAccel* accel_device_view(enc_accel a);
 struct WaveScratch {
   float* rays[2] = {nullptr, nullptr};
   uint32_t* path[2] = {nullptr, nullptr};
+  float* srays[2] = {nullptr, nullptr};    // shadow-photon rays
+  uint32_t* spath[2] = {nullptr, nullptr};
   void* hits = nullptr;
-  uint32_t* counters = nullptr;  // device: stored photons, next wave's rays
-  uint32_t* h_counts = nullptr;  // pinned host copy of the two counters
+  uint32_t* counters = nullptr;  // device: photons offered per store, next wave's and
+                                 // next shadow wave's rays, shadow rays dropped
+  uint32_t* h_counts = nullptr;  // pinned host copy of the counters
   size_t cap = 0;                // photons the buffers hold
   std::mutex mu;
 };

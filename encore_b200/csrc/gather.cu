@@ -60,6 +60,7 @@ struct GatherParams {
   int32_t* count;
   uint32_t* status;
   uint32_t* counter;  // this launch's query-queue head, zeroed before it
+  uint32_t* visits;   // COUNT: 4 words per query (see gather_kernel)
   unsigned nq;
   int k;
   float r2max;
@@ -118,7 +119,11 @@ __device__ __forceinline__ void warp_max(const float (&dd)[S], int lane, int lim
   v = l1 == 0 ? -INFINITY : __uint_as_float(mv);
 }
 
-template <int S, bool NEAREST>
+// COUNT: also records per query the work behind the roofline's bytes:
+// visits[4q] child boxes tested (24 bytes each), [4q+1] photons tested (a
+// 16-byte position each), [4q+2] normals read (16 bytes each), [4q+3]
+// photons found (their 16-byte power is read by the estimate).
+template <int S, bool NEAREST, bool COUNT = false>
 __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
   // stack entries, their squared distances, and a leaf entry's photon count
   __shared__ uint32_t s_item[kWarpsPerBlock][kStack];
@@ -172,6 +177,7 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
     }
     __syncwarp();
     unsigned steps = 0;
+    uint32_t n_box = 0, n_pos = 0, n_nrm = 0;
     while (sp > 0) {
       if (++steps > kMaxSteps) {
         if (lane == 0) atomicOr(P.status, 1u);
@@ -206,6 +212,7 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
           pass = cd < r2;
         }
         const unsigned m = __ballot_sync(kFull, pass);
+        if (COUNT) n_box += __popc(__ballot_sync(kFull, child < P.lvl_count[cl]));
         const int n = __popc(m);
         if (sp + n > kStack) {
           if (lane == 0) atomicOr(P.status, 2u);
@@ -247,6 +254,9 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
       bool acc = false;
       float d2 = 0.f;
       int orig = -1;
+      if (COUNT) {
+        n_pos += (uint32_t)(c0 + c1);
+      }
       if (lane < c0 + c1) {
         const float4 p = __ldg(P.pos4 + pidx);
         const float x = fs(qx, p.x), y = fs(qy, p.y), z = fs(qz, p.z);
@@ -258,6 +268,8 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
           acc = (pn.x == nx) && (pn.y == ny) && (pn.z == nz);
         }
       }
+      if (COUNT && !P.ignore_normal)
+        n_nrm += __popc(__ballot_sync(kFull, lane < c0 + c1 && d2 < r2));
       unsigned m = __ballot_sync(kFull, acc);
       if (m && count < k) {
         // fill free heap slots in one step: the accepted candidate of rank r
@@ -374,14 +386,20 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
         P.rgb[3 * (size_t)q + 2] = B;
       }
     }
+    if (COUNT && lane == 0) {
+      P.visits[4 * (size_t)q] = n_box;
+      P.visits[4 * (size_t)q + 1] = n_pos;
+      P.visits[4 * (size_t)q + 2] = n_nrm;
+      P.visits[4 * (size_t)q + 3] = (uint32_t)count;
+    }
     ++q;
   }
 }
 
-template <bool NEAREST>
+template <bool NEAREST, bool COUNT = false>
 int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, size_t nq, int k,
                   float max_dist, int flags, float* rgb, int32_t* idx, float* d2, int32_t* count,
-                  cudaStream_t s) {
+                  cudaStream_t s, uint32_t* visits = nullptr) {
   if (nq == 0) return 0;
   GatherParams p;
   p.box = m.d_box;
@@ -401,6 +419,7 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
   p.idx = idx;
   p.d2 = d2;
   p.count = count;
+  p.visits = visits;
   p.status = m.d_status;
   const uint32_t slot = __atomic_fetch_add(const_cast<uint32_t*>(&m.counter_seq), 1u,
                                            __ATOMIC_RELAXED) % kGatherSlots;
@@ -411,10 +430,10 @@ int launch_gather(const DevPhotonMap& m, const float* qpos, const float* qnrm, s
   p.ignore_normal = (flags & ENC_GATHER_IGNORE_NORMAL) ? 1 : 0;
   p.caustic = m.caustic;
   const int S = k <= 32 ? 1 : (k <= 64 ? 2 : (k <= 128 ? 4 : 8));
-  void (*kern)(GatherParams) = S == 1   ? gather_kernel<1, NEAREST>
-                               : S == 2 ? gather_kernel<2, NEAREST>
-                               : S == 4 ? gather_kernel<4, NEAREST>
-                                        : gather_kernel<8, NEAREST>;
+  void (*kern)(GatherParams) = S == 1   ? gather_kernel<1, NEAREST, COUNT>
+                               : S == 2 ? gather_kernel<2, NEAREST, COUNT>
+                               : S == 4 ? gather_kernel<4, NEAREST, COUNT>
+                                        : gather_kernel<8, NEAREST, COUNT>;
   // One resident wave of persistent warps (the register count allows 5
   // blocks of 256 threads per SM): a larger grid would only queue blocks
   // that find the query queue empty.
@@ -438,6 +457,13 @@ int launch_radiance(const DevPhotonMap& m, const float* d_qpos, const float* d_q
                     int k, float max_dist, int flags, float* d_rgb, void* stream) {
   return launch_gather<false>(m, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, nullptr, nullptr,
                               nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int launch_radiance_counted(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm,
+                            size_t nq, int k, float max_dist, int flags, float* d_rgb,
+                            uint32_t* d_visits, void* stream) {
+  return launch_gather<false, true>(m, d_qpos, d_qnrm, nq, k, max_dist, flags, d_rgb, nullptr,
+                                    nullptr, nullptr, static_cast<cudaStream_t>(stream), d_visits);
 }
 
 int launch_nearest(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,

@@ -65,7 +65,8 @@ struct DevPhotonMap {
   float* d_pow4 = nullptr;
   uint32_t* d_status = nullptr;
   // Query-queue heads: each launch takes the next of kGatherSlots words and
-  // zeroes it on its stream, so launches on different streams never share one.
+  // zeroes it on its stream, so up to kGatherSlots launches in flight at once
+  // never share one (the next launch after those reuses the first's head).
   uint32_t* d_counter = nullptr;
   uint32_t counter_seq = 0;
   uint32_t nnodes = 0;
@@ -78,6 +79,11 @@ struct DevPhotonMap {
 // Launchers (gather.cu).  k <= 256.  Asynchronous on `stream`.
 int launch_radiance(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
                     int k, float max_dist, int flags, float* d_rgb, void* stream);
+// The radiance launch that also writes 4 counters per query (gather.cu:
+// child boxes tested, photons tested, normals read, photons found).
+int launch_radiance_counted(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm,
+                            size_t nq, int k, float max_dist, int flags, float* d_rgb,
+                            uint32_t* d_visits, void* stream);
 int launch_nearest(const DevPhotonMap& m, const float* d_qpos, const float* d_qnrm, size_t nq,
                    int k, float max_dist, int flags, int32_t* d_idx, float* d_d2,
                    int32_t* d_count, void* stream);

@@ -1,15 +1,18 @@
 // Serving loop: resident scene pool, admission by slot capacity and HBM
 // budget, continuous batching into fused multi-scene launches.
 //
-// Threads.  submit() only queues.  The scheduler thread waits for a free
-// slot and queued requests, admits requests in arrival order while they fit
-// the slot's ray capacity, and enqueues on the slot's stream: the rays' copies
-// in, the batch tables, one multi-scene closest-hit launch and one any-hit
-// launch, the result copies out, the status word, and an event.  It then goes
-// back for the next group at once, so requests that arrive while a group is
-// on the GPU form the next group and run alongside it on another stream.
-// The completion thread polls the in-flight events, stamps each finished
-// request and frees its slot.  Waiters block on a condition variable.
+// Threads.  submit() only queues: a request is split into pieces of at most
+// a slot's ray capacity, so a request larger than one slot runs over several
+// rounds.  The scheduler thread waits for a free slot and queued pieces,
+// admits pieces in arrival order while they fit the slot's ray capacity, and
+// enqueues on the slot's stream: the rays' copies in, the batch tables, one
+// multi-scene closest-hit launch and one any-hit launch, the result copies
+// out, one status word per piece, and an event.  It then goes back for the
+// next group at once, so requests that arrive while a group is on the GPU
+// form the next group and run alongside it on another stream.  The
+// completion thread polls the in-flight events, stamps each piece's request
+// (done once its last piece is; failed if any piece failed) and frees the
+// slot.  Waiters block on a condition variable.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,8 +47,16 @@ struct Request {
   void* out = nullptr;
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = ENC_OK;
-  bool running = false;
+  uint32_t pieces_left = 0;  // pieces not finished yet
+  bool running = false;      // some piece has been admitted
   bool done = false;
+};
+
+// A contiguous range of a request's rays that fits one slot.
+struct Piece {
+  Request* r = nullptr;
+  uint64_t off = 0;
+  uint64_t n = 0;
 };
 
 struct Slot {
@@ -55,12 +66,21 @@ struct Slot {
   char* d_out = nullptr;     // capacity * 16 bytes
   BatchDesc* d_tab = nullptr;  // closest table, then any table (kMaxReqPerSlot each)
   uint32_t* d_starts = nullptr;
-  uint32_t* d_words = nullptr;  // queue head closest, queue head any, status
+  uint32_t* d_words = nullptr;  // queue head closest, queue head any
+  uint32_t* d_bstat = nullptr;  // per-piece status: closest pieces, then any pieces
   BatchDesc* h_tab = nullptr;   // pinned staging of the tables
   uint32_t* h_starts = nullptr;
-  uint32_t* h_status = nullptr;
-  std::vector<Request*> reqs;
+  uint32_t* h_bstat = nullptr;  // pinned copy of the per-piece status words
+  bool failed = false;          // the round could not be enqueued
+  std::vector<Piece> pieces;
+  std::vector<uint32_t> piece_word;  // each piece's index into h_bstat
   bool busy = false;
+};
+
+// Scene-table facts a round needs, read under the server lock when the
+// round is formed (enc_server_add_scene writes them under the same lock).
+struct RoundView {
+  int width = 8, predicate = 0, depth = 8;
 };
 
 }  // namespace
@@ -80,7 +100,7 @@ struct enc_server_s {
   std::vector<Slot> slots;
   std::mutex mu;
   std::condition_variable cv_sched, cv_done;
-  std::deque<Request*> pending;
+  std::deque<Piece> pending;
   std::deque<int> inflight;
   std::unordered_map<uint64_t, Request*> reqs;
   uint64_t next_id = 1;
@@ -90,7 +110,7 @@ struct enc_server_s {
 
 namespace {
 
-cudaError_t enqueue_round(enc_server S, Slot& sl) {
+cudaError_t enqueue_round(enc_server S, Slot& sl, const RoundView& v) {
   const uint32_t chunk = (uint32_t)S->L.chunk;
   uint64_t off = 0;
   uint32_t nc = 0, na = 0;
@@ -100,23 +120,28 @@ cudaError_t enqueue_round(enc_server S, Slot& sl) {
   uint32_t* sc = sl.h_starts;
   uint32_t* sa = sl.h_starts + kMaxReqPerSlot + 1;
   cudaError_t e = cudaSuccess;
-  for (Request* r : sl.reqs) {
-    e = cudaMemcpyAsync(sl.d_rays + off * 32, r->rays, r->n * 32, cudaMemcpyHostToDevice, sl.s);
+  sl.piece_word.clear();
+  for (const Piece& pc : sl.pieces) {
+    const Request* r = pc.r;
+    e = cudaMemcpyAsync(sl.d_rays + off * 32, r->rays + 8 * pc.off, pc.n * 32,
+                        cudaMemcpyHostToDevice, sl.s);
     if (e != cudaSuccess) return e;
     BatchDesc d{reinterpret_cast<const float*>(sl.d_rays + off * 32), sl.d_out + off * 16,
-                r->scene, (uint32_t)r->n, 0, (uint32_t)r->kind};
+                r->scene, (uint32_t)pc.n, 0, (uint32_t)r->kind};
     if (r->kind == ENC_REQ_CLOSEST) {
       d.start = (uint32_t)qc;
       sc[nc] = (uint32_t)qc;
+      sl.piece_word.push_back(nc);
       tc[nc++] = d;
-      qc += (r->n + chunk - 1) / chunk * chunk;
+      qc += (pc.n + chunk - 1) / chunk * chunk;
     } else {
       d.start = (uint32_t)qa;
       sa[na] = (uint32_t)qa;
+      sl.piece_word.push_back(kMaxReqPerSlot + na);
       ta[na++] = d;
-      qa += (r->n + chunk - 1) / chunk * chunk;
+      qa += (pc.n + chunk - 1) / chunk * chunk;
     }
-    off += r->n;
+    off += pc.n;
   }
   sc[nc] = (uint32_t)qc;
   sa[na] = (uint32_t)qa;
@@ -125,13 +150,14 @@ cudaError_t enqueue_round(enc_server S, Slot& sl) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(sl.d_starts, sl.h_starts, 2 * (kMaxReqPerSlot + 1) * sizeof(uint32_t),
                         cudaMemcpyHostToDevice, sl.s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_bstat, 0, 2 * kMaxReqPerSlot * 4, sl.s);
   if (e != cudaSuccess) return e;
   MultiLaunch m;
   m.d_scenes = S->d_scenes;
-  m.width = S->width;
-  m.predicate = S->predicate;
+  m.width = v.width;
+  m.predicate = v.predicate;
   m.device = S->device;
-  m.stack_depth = S->depth;
+  m.stack_depth = v.depth;
   m.d_status = sl.d_words + 2;
   if (nc) {
     m.d_batches = sl.d_tab;
@@ -139,6 +165,7 @@ cudaError_t enqueue_round(enc_server S, Slot& sl) {
     m.nbatches = nc;
     m.total = (uint32_t)qc;
     m.d_counter = sl.d_words;
+    m.d_batch_status = sl.d_bstat;
     int le = launch_multi_closest(m, S->L, sl.s);
     if (le) return (cudaError_t)le;
   }
@@ -148,18 +175,20 @@ cudaError_t enqueue_round(enc_server S, Slot& sl) {
     m.nbatches = na;
     m.total = (uint32_t)qa;
     m.d_counter = sl.d_words + 1;
+    m.d_batch_status = sl.d_bstat + kMaxReqPerSlot;
     int le = launch_multi_any(m, S->L, sl.s);
     if (le) return (cudaError_t)le;
   }
   off = 0;
-  for (Request* r : sl.reqs) {
-    const size_t bytes = r->n * (r->kind == ENC_REQ_CLOSEST ? sizeof(enc_hit) : 1);
-    e = cudaMemcpyAsync(r->out, sl.d_out + off * 16, bytes, cudaMemcpyDeviceToHost, sl.s);
+  for (const Piece& pc : sl.pieces) {
+    const Request* r = pc.r;
+    const size_t rec = r->kind == ENC_REQ_CLOSEST ? sizeof(enc_hit) : 1;
+    e = cudaMemcpyAsync(static_cast<char*>(r->out) + pc.off * rec, sl.d_out + off * 16,
+                        pc.n * rec, cudaMemcpyDeviceToHost, sl.s);
     if (e != cudaSuccess) return e;
-    off += r->n;
+    off += pc.n;
   }
-  e = cudaMemcpyAsync(sl.h_status, sl.d_words + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, sl.s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_words + 2, 0, sizeof(uint32_t), sl.s);
+  e = cudaMemcpyAsync(sl.h_bstat, sl.d_bstat, 2 * kMaxReqPerSlot * 4, cudaMemcpyDeviceToHost, sl.s);
   if (e == cudaSuccess) e = cudaEventRecord(sl.ev, sl.s);
   return e;
 }
@@ -181,28 +210,32 @@ void sched_loop(enc_server S) {
     });
     if (S->stop) return;
     Slot& sl = S->slots[si];
-    sl.reqs.clear();
+    sl.pieces.clear();
+    sl.failed = false;
     uint64_t used = 0;
     const double t = steady_now();
-    while (!S->pending.empty() && sl.reqs.size() < kMaxReqPerSlot) {
-      Request* r = S->pending.front();
-      if (used + r->n > S->capacity) break;  // next group; arrival order is kept
+    while (!S->pending.empty() && sl.pieces.size() < kMaxReqPerSlot) {
+      const Piece pc = S->pending.front();
+      if (used + pc.n > S->capacity) break;  // next group; arrival order is kept
       S->pending.pop_front();
-      r->running = true;
-      r->t_start = t;
-      sl.reqs.push_back(r);
-      used += r->n;
+      if (!pc.r->running) {
+        pc.r->running = true;
+        pc.r->t_start = t;
+      }
+      sl.pieces.push_back(pc);
+      used += pc.n;
     }
-    if (sl.reqs.empty()) continue;
+    if (sl.pieces.empty()) continue;
+    const RoundView v{S->width, S->predicate, S->depth};
     sl.busy = true;
     lk.unlock();
-    cudaError_t e = enqueue_round(S, sl);
+    cudaError_t e = enqueue_round(S, sl, v);
     lk.lock();
     if (e != cudaSuccess) {
       set_error(std::string("server round: ") + cudaGetErrorString(e));
-      // let the completion thread finish these requests with an error once
+      // let the completion thread finish these pieces with an error once
       // whatever was enqueued has drained
-      *sl.h_status = 0x80000000u;
+      sl.failed = true;
       cudaEventRecord(sl.ev, sl.s);
     }
     S->inflight.push_back(si);
@@ -228,18 +261,19 @@ void comp_loop(enc_server S) {
     lk.lock();
     for (auto& f : finished) {
       Slot& sl = S->slots[f.first];
-      int st = ENC_OK;
-      if (f.second != cudaSuccess) st = ENC_ERR_CUDA;
-      else if (*sl.h_status & 0x80000000u) st = ENC_ERR_CUDA;
-      else if (*sl.h_status) st = ENC_ERR_WATCHDOG;
-      for (Request* r : sl.reqs) {
-        r->t_done = t;
-        r->status = st;
-        r->done = true;
+      for (size_t i = 0; i < sl.pieces.size(); ++i) {
+        Request* r = sl.pieces[i].r;
+        int st = ENC_OK;
+        if (f.second != cudaSuccess || sl.failed) st = ENC_ERR_CUDA;
+        else if (i < sl.piece_word.size() && sl.h_bstat[sl.piece_word[i]]) st = ENC_ERR_WATCHDOG;
+        if (st != ENC_OK && r->status == ENC_OK) r->status = st;
+        if (--r->pieces_left == 0) {
+          r->t_done = t;
+          r->done = true;
+        }
       }
-      sl.reqs.clear();
+      sl.pieces.clear();
       sl.busy = false;
-      *sl.h_status = 0;
       S->inflight.erase(std::find(S->inflight.begin(), S->inflight.end(), f.first));
     }
     if (!finished.empty()) {
@@ -258,9 +292,10 @@ void free_slots(enc_server S) {
     cudaFree(sl.d_tab);
     cudaFree(sl.d_starts);
     cudaFree(sl.d_words);
+    cudaFree(sl.d_bstat);
     cudaFreeHost(sl.h_tab);
     cudaFreeHost(sl.h_starts);
-    cudaFreeHost(sl.h_status);
+    cudaFreeHost(sl.h_bstat);
   }
   S->slots.clear();
   cudaFree(S->d_scenes);
@@ -301,7 +336,7 @@ enc_status enc_server_create(const enc_server_opts* opts, enc_server* out) {
     set_error("enc_server_create: launch options out of range");
     return ENC_ERR_INVALID_ARG;
   }
-  const uint64_t per_slot = o.slot_rays * 48 + 2 * kMaxReqPerSlot * (sizeof(BatchDesc) + 4) + 64;
+  const uint64_t per_slot = o.slot_rays * 48 + 2 * kMaxReqPerSlot * (sizeof(BatchDesc) + 8) + 64;
   S->slot_bytes = per_slot * o.slots + kMaxScenes * sizeof(SceneDesc);
   if (S->slot_bytes > o.budget_bytes) {
     delete S;
@@ -322,10 +357,10 @@ enc_status enc_server_create(const enc_server_opts* opts, enc_server* out) {
     if (e == cudaSuccess) e = cudaMalloc((void**)&sl.d_starts, 2 * (kMaxReqPerSlot + 1) * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&sl.d_words, 16);
     if (e == cudaSuccess) e = cudaMemset(sl.d_words, 0, 16);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&sl.d_bstat, 2 * kMaxReqPerSlot * 4);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&sl.h_tab, 2 * kMaxReqPerSlot * sizeof(BatchDesc));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&sl.h_starts, 2 * (kMaxReqPerSlot + 1) * 4);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&sl.h_status, 4);
-    if (e == cudaSuccess) *sl.h_status = 0;
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&sl.h_bstat, 2 * kMaxReqPerSlot * 4);
   }
   if (e != cudaSuccess) {
     set_error(std::string("enc_server_create: ") + cudaGetErrorString(e));
@@ -400,11 +435,6 @@ enc_status enc_server_submit(enc_server S, uint32_t scene_id, int32_t kind, cons
     set_error("enc_server_submit: unknown scene");
     return ENC_ERR_INVALID_ARG;
   }
-  if (nrays > S->capacity) {
-    delete r;
-    set_error("enc_server_submit: request larger than a slot's ray capacity");
-    return ENC_ERR_BUDGET;
-  }
   r->id = S->next_id++;
   S->reqs[r->id] = r;
   *request_id = r->id;
@@ -414,7 +444,15 @@ enc_status enc_server_submit(enc_server S, uint32_t scene_id, int32_t kind, cons
     S->cv_done.notify_all();
     return ENC_OK;
   }
-  S->pending.push_back(r);
+  // pieces of at most one slot's capacity, queued back to back
+  for (uint64_t off = 0; off < nrays; off += S->capacity) {
+    Piece pc;
+    pc.r = r;
+    pc.off = off;
+    pc.n = std::min<uint64_t>(S->capacity, nrays - off);
+    S->pending.push_back(pc);
+    ++r->pieces_left;
+  }
   S->cv_sched.notify_all();
   return ENC_OK;
 }
@@ -457,7 +495,10 @@ enc_status enc_server_cancel(enc_server S, uint64_t id) {
   Request* r = it->second;
   if (r->done) return ENC_OK;
   if (r->running) return ENC_ERR_NOT_READY;
-  S->pending.erase(std::find(S->pending.begin(), S->pending.end(), r));
+  S->pending.erase(std::remove_if(S->pending.begin(), S->pending.end(),
+                                  [&](const Piece& pc) { return pc.r == r; }),
+                   S->pending.end());
+  r->pieces_left = 0;
   r->status = ENC_ERR_CANCELLED;
   r->done = true;
   r->t_start = r->t_done = steady_now();

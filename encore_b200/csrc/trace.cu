@@ -115,6 +115,7 @@ struct TraceParams {
   const uint8_t* nodes;
   const float4* tris;  // 3 per triangle
   const float4* rays;  // 2 per ray
+  const uint32_t* order;  // null, or: queue index q traces ray order[q] (binned batches)
   void* out;           // enc_hit* (closest) or uint8_t* (any)
   uint32_t* visits;    // COUNT: 2 per ray
   unsigned* counter;
@@ -129,6 +130,7 @@ struct TraceParams {
   const BatchDesc* batches;
   const uint32_t* starts;  // nbatches + 1 chunk-aligned queue offsets
   unsigned nbatches;
+  uint32_t* batch_status;  // MULTI: one status word per batch, or null (all in *status)
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -222,6 +224,12 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
   // Warp-private ray pool [pool_next, pool_end), refilled in chunks.
   unsigned pool_next = 0, pool_end = 0;
   bool exhausted = false;
+  // Binned batches: lane j holds order[pool_base + j] of the current chunk,
+  // loaded once when the chunk is taken (one coalesced load per chunk instead
+  // of a dependent load per refill); chunks above 32 rays read the rest
+  // directly.
+  constexpr bool kOrdered = !MULTI && !ANY;  // binned batches: closest hit only
+  unsigned pool_base = 0, ord_reg = 0;
 
   int ray = -1;
   float ox = 0, oy = 0, oz = 0, dx = 0, dy = 0, dz = 0, ix = 0, iy = 0, iz = 0, tmin = 0, tmax = 0;
@@ -239,6 +247,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
   void* l_out = P.out;
   unsigned l_idx = 0;          // index of the ray in its output array
   unsigned pool_batch = 0;     // MULTI: batch of the current pool
+  uint32_t* l_status = P.status;  // the status word of the lane's ray (MULTI: its batch's)
 
   while (true) {
     // ---- refill idle lanes from the warp pool --------------------------
@@ -253,6 +262,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
           break;
         }
         pool_next = b;
+        pool_base = b;
+        if (kOrdered && P.order != nullptr && b + lane < P.nrays) ord_reg = __ldg(P.order + b + lane);
         if constexpr (MULTI) {
           // batch = last start <= b (starts are chunk-aligned, so the whole
           // chunk lies in it); its real rays end before the padding
@@ -270,8 +281,12 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
       }
       const unsigned avail = pool_end > pool_next ? pool_end - pool_next : 0u;
       const unsigned rank = __popc(need & lt);
+      const unsigned qoff = pool_next - pool_base + rank;  // offset of this lane's ray in the chunk
+      const unsigned via = kOrdered ? __shfl_sync(kFull, ord_reg, qoff & 31u) : 0u;
       if (((need >> lane) & 1u) && rank < avail) {
         ray = (int)(pool_next + rank);
+        if (kOrdered && P.order != nullptr)
+          ray = (int)(qoff < 32u ? via : __ldg(P.order + pool_next + rank));
         const float4* rp;
         if constexpr (MULTI) {
           const BatchDesc& bd = P.batches[pool_batch];
@@ -282,6 +297,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
           l_tris = reinterpret_cast<const float4*>(sd.tris);
           l_nnodes = sd.nnodes;
           l_ntris = sd.ntris;
+          if (P.batch_status) l_status = P.batch_status + pool_batch;
           rp = reinterpret_cast<const float4*>(bd.rays) + 2 * (size_t)l_idx;
         } else {
           l_idx = (unsigned)ray;
@@ -331,11 +347,11 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
     uint32_t tmask = 0, tbase = 0;  // triangles of the node's hit leaves
     if (ray >= 0) {
       if (++steps > kMaxSteps) {
-        atomicOr(P.status, kStatusWatchdog);
+        atomicOr(l_status, kStatusWatchdog);
         best_id = -1;
         done = true;
       } else if (node >= l_nnodes) {
-        atomicOr(P.status, kStatusBounds);
+        atomicOr(l_status, kStatusBounds);
         best_id = -1;
         done = true;
       } else {
@@ -462,7 +478,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             const uint32_t rest = hitk & (hitk - 1u);
             if (rest) {
               if (sp >= P.stack_depth) {
-                atomicOr(P.status, kStatusStack);
+                atomicOr(l_status, kStatusStack);
                 best_id = -1;
                 done = true;
               } else {
@@ -486,7 +502,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             node = child_base + rnk[0];
             if (nh > 1) {
               if (sp >= P.stack_depth) {
-                atomicOr(P.status, kStatusStack);
+                atomicOr(l_status, kStatusStack);
                 best_id = -1;
                 done = true;
               } else {
@@ -512,7 +528,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
           trimask &= trimask - 1;
           const uint32_t ti = tri_base + k;
           if (ti >= l_ntris) {
-            atomicOr(P.status, kStatusBounds);
+            atomicOr(l_status, kStatusBounds);
             continue;
           }
           const float4* tp = l_tris + 3 * (size_t)ti;
@@ -586,10 +602,13 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         const int wbid = __shfl_sync(kFull, best_id, own);
         const float4* wtris = l_tris;
         unsigned wntris = l_ntris;
+        uint32_t* wstatus = P.status;
         if constexpr (MULTI) {
           const unsigned long long tp = __shfl_sync(kFull, (unsigned long long)l_tris, own);
           wtris = reinterpret_cast<const float4*>(tp);
           wntris = __shfl_sync(kFull, l_ntris, own);
+          wstatus = reinterpret_cast<uint32_t*>(
+              __shfl_sync(kFull, (unsigned long long)l_status, own));
         }
         bool cand = false;
         unsigned long long ckey = 0;
@@ -597,7 +616,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         if ((int)lane < nitems) {
           const uint32_t ti = it_tri[lane];
           if (ti >= wntris) {
-            atomicOr(P.status, kStatusBounds);
+            atomicOr(wstatus, kStatusBounds);
           } else {
             const float4* tp = wtris + 3 * (size_t)ti;
             const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -854,11 +873,12 @@ constexpr size_t stack_entry_bytes(int W) {
 
 template <int W, bool CLAMP, bool ANY, bool COUNT>
 int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t* visits,
-             const Launch& L, cudaStream_t s) {
+             const Launch& L, cudaStream_t s, const uint32_t* order) {
   TraceParams p{};
   p.nodes = static_cast<const uint8_t*>(a.d_nodes);
   p.tris = reinterpret_cast<const float4*>(a.d_tris);
   p.rays = reinterpret_cast<const float4*>(rays);
+  p.order = order;
   p.out = out;
   p.visits = visits;
   const uint32_t slot =
@@ -889,18 +909,18 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
 
 template <bool ANY, bool COUNT>
 int dispatch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t* visits,
-               const Launch& L, cudaStream_t s) {
+               const Launch& L, cudaStream_t s, const uint32_t* order = nullptr) {
   const bool clamp = a.predicate == ENC_PRED_REFERENCE;
   switch (a.width) {
     case 2:
-      return clamp ? launch_w<2, true, ANY, COUNT>(a, rays, n, out, visits, L, s)
-                   : launch_w<2, false, ANY, COUNT>(a, rays, n, out, visits, L, s);
+      return clamp ? launch_w<2, true, ANY, COUNT>(a, rays, n, out, visits, L, s, order)
+                   : launch_w<2, false, ANY, COUNT>(a, rays, n, out, visits, L, s, order);
     case 4:
-      return clamp ? launch_w<4, true, ANY, COUNT>(a, rays, n, out, visits, L, s)
-                   : launch_w<4, false, ANY, COUNT>(a, rays, n, out, visits, L, s);
+      return clamp ? launch_w<4, true, ANY, COUNT>(a, rays, n, out, visits, L, s, order)
+                   : launch_w<4, false, ANY, COUNT>(a, rays, n, out, visits, L, s, order);
     default:
-      return clamp ? launch_w<8, true, ANY, COUNT>(a, rays, n, out, visits, L, s)
-                   : launch_w<8, false, ANY, COUNT>(a, rays, n, out, visits, L, s);
+      return clamp ? launch_w<8, true, ANY, COUNT>(a, rays, n, out, visits, L, s, order)
+                   : launch_w<8, false, ANY, COUNT>(a, rays, n, out, visits, L, s, order);
   }
 }
 
@@ -947,12 +967,12 @@ int device_sm_count(int device) {
 }
 
 int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_hits,
-                   const Launch& L, void* stream, uint32_t* d_visits) {
+                   const Launch& L, void* stream, uint32_t* d_visits, const uint32_t* d_order) {
   if (n == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (a.kind == ENC_ACCEL_KDTREE) return launch_kd<false>(a, d_rays, n, d_hits, s);
-  if (d_visits) return dispatch_w<false, true>(a, d_rays, n, d_hits, d_visits, L, s);
-  return dispatch_w<false, false>(a, d_rays, n, d_hits, nullptr, L, s);
+  if (d_visits) return dispatch_w<false, true>(a, d_rays, n, d_hits, d_visits, L, s, d_order);
+  return dispatch_w<false, false>(a, d_rays, n, d_hits, nullptr, L, s, d_order);
 }
 
 int launch_any(const DevAccel& a, const float* d_rays, size_t n, uint8_t* d_occ, const Launch& L,
@@ -996,6 +1016,31 @@ int launch_w_external(const DevAccel& a, const float* rays, size_t n, enc_hit* h
 
 }  // namespace
 
+int warm_closest_kernel(const DevAccel& a, uint32_t* counter, uint32_t* status) {
+  // An empty batch: every warp finds the queue exhausted at once.  The launch
+  // loads the kernel's module and sizes the context's local memory for it.
+  Launch L = resolve_launch(nullptr, a.kind, a.width);
+  L.blocks_per_sm = 1;
+  int e = 0;
+  const bool clamp = a.predicate == ENC_PRED_REFERENCE;
+  float* no_rays = nullptr;
+  switch (a.width) {
+    case 2:
+      e = clamp ? launch_w_external<2, true>(a, no_rays, 0, nullptr, L, 0, counter, status)
+                : launch_w_external<2, false>(a, no_rays, 0, nullptr, L, 0, counter, status);
+      break;
+    case 4:
+      e = clamp ? launch_w_external<4, true>(a, no_rays, 0, nullptr, L, 0, counter, status)
+                : launch_w_external<4, false>(a, no_rays, 0, nullptr, L, 0, counter, status);
+      break;
+    default:
+      e = clamp ? launch_w_external<8, true>(a, no_rays, 0, nullptr, L, 0, counter, status)
+                : launch_w_external<8, false>(a, no_rays, 0, nullptr, L, 0, counter, status);
+  }
+  if (e != 0) return e;
+  return (int)cudaStreamSynchronize(0);
+}
+
 int launch_closest_external_scratch(const DevAccel& a, const float* d_rays, size_t n,
                                     enc_hit* d_hits, const Launch& L, void* stream,
                                     uint32_t* counter, uint32_t* status) {
@@ -1032,6 +1077,7 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   p.batches = m.d_batches;
   p.starts = m.d_starts;
   p.nbatches = m.nbatches;
+  p.batch_status = m.d_batch_status;
   size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
   auto k = wbvh_trace<W, CLAMP, ANY, false, true>;
   if (smem > 48 * 1024) {

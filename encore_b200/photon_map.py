@@ -90,6 +90,23 @@ class PhotonMap:
                                                      ptr(d_rgb), stream),
               "enc_photonmap_radiance_device")
 
+    def count_visits(self, n: int, max_distance: float, d_q, d_n, nq: int, d_rgb, d_visits,
+                     ignore_normal: bool = False, stream=None) -> None:
+        """The device radiance estimate with per-query work counters (4 words
+        per query: child boxes tested, photons tested, normals read, photons
+        found), for the bytes-per-query roofline."""
+        self.balance_and_construct()
+        check(self.lib.enc_photonmap_count_visits(self.handle, ptr(d_q), ptr(d_n), nq, n,
+                                                  max_distance, self._flags(ignore_normal),
+                                                  ptr(d_rgb), ptr(d_visits), stream),
+              "enc_photonmap_count_visits")
+
+    def check(self, stream=None) -> None:
+        """Waits for `stream` and raises if a gather on this map stopped at
+        its loop bound (the device form does not read the status itself)."""
+        stream = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        check(self.lib.enc_photonmap_check(self.handle, stream), "enc_photonmap_check")
+
     # PhotonMap::GetNearestNPhotons (PhotonMap.cpp:76-94), batched; ascending distance
     def get_nearest_n_photons(self, n: int, max_distance: float, location, normal,
                               ignore_normal: bool = False):

@@ -47,6 +47,29 @@ def trace_photons(acc: Accelerator, light_center, light_size: float, nphotons: i
     return stored.value
 
 
+def trace_photon_maps(acc: Accelerator, light_center, light_size: float, nphotons: int,
+                      direct, indirect, max_bounces: int = 3, albedo: float = 0.7, seed: int = 1,
+                      emit_offset: float = 0.01, bounce_offset: float = 0.001,
+                      shadow_offset: float = 0.0, fill_indirect: bool = False,
+                      stream=None) -> tuple[int, int, int]:
+    """The reference's direct / indirect map split (enc_photons_trace_maps_device).
+    `direct` and `indirect` are (pos, nrm, pow, tag) tuples of CUDA tensors
+    ((cap, 3) float32 x 3 and (cap,) int32, or None for no tags).  Returns
+    (stored direct, stored indirect, paths emitted)."""
+    def store(t):
+        pos, nrm, pw, tag = t
+        return _lib.PhotonStore(ptr(pos), ptr(nrm), ptr(pw), ptr(tag), int(pos.shape[0]))
+    o = _lib.PhotonOpts((C.c_float * 3)(*light_center), light_size, nphotons, max_bounces, albedo,
+                        seed, emit_offset, bounce_offset)
+    sd, si = store(direct), store(indirect)
+    stored = (C.c_uint32 * 2)()
+    emitted = C.c_uint32()
+    check(_lib.load().enc_photons_trace_maps_device(
+        acc.handle, C.byref(o), shadow_offset, int(fill_indirect), C.byref(sd), C.byref(si),
+        stored, C.byref(emitted), _stream_ptr(stream)), "enc_photons_trace_maps_device")
+    return stored[0], stored[1], emitted.value
+
+
 def photon_map_from_device(d_pos, d_nrm, d_pow, n: int, caustic: bool = False,
                            device: int = 0) -> PhotonMap:
     pm = PhotonMap(n, caustic=caustic, device=device)

@@ -198,10 +198,42 @@ enc_status enc_accel_info_get(enc_accel accel, enc_accel_info* info);
 enc_status enc_intersect_closest(enc_accel accel, const float* rays, size_t nrays, enc_hit* hits,
                                  const enc_launch_opts* launch, enc_stream stream);
 /* Device-buffer form: rays and hits already in device memory; asynchronous
- * on `stream`.  Kernel status is checked by enc_stream_check. */
+ * on `stream`.  Kernel status is read by enc_accel_check.  Each launch on an
+ * accelerator takes the next of its 256 work-queue heads, so at most 256
+ * launches on one accelerator may be in flight together; a launch captured
+ * into a CUDA graph keeps the head it was captured with. */
 enc_status enc_intersect_closest_device(enc_accel accel, const float* d_rays, size_t nrays,
                                         enc_hit* d_hits, const enc_launch_opts* launch,
                                         enc_stream stream);
+
+/* Binned closest hit, device buffers.  The same results as
+ * enc_intersect_closest_device, bit for bit; the batch is first binned by a
+ * key of each ray's origin cell and direction cell (a counting sort into a
+ * permutation in `d_scratch`), and the traversal takes its rays in that
+ * order, so the rays of a warp walk similar paths through the tree.  Hits are
+ * written at each ray's own index.  Pays for incoherent batches (shuffled
+ * bounces); the binning costs three streaming passes over the rays.
+ *
+ * The key interleaves `origin_bits` bits of the origin cell (over the scene
+ * box; bits go to the axis with the widest cells first) with `dir_bits` bits
+ * of the direction's octahedral coordinates.  origin_bits + dir_bits <= 20;
+ * both 0 = the tuned default.  probe_frac > 0 bins the point
+ * o + probe_frac * |scene diagonal| * d instead of the origin.
+ *
+ * d_scratch: device memory of at least enc_bin_scratch_bytes() bytes,
+ * 256-byte aligned, owned by the caller and used on `stream` only until the
+ * launch completes (calls that share one scratch buffer must be ordered on
+ * one stream).  No counterpart in the reference (one ray per call). */
+typedef struct enc_bin_opts {
+  int32_t origin_bits;
+  int32_t dir_bits;
+  float probe_frac;
+} enc_bin_opts;
+enc_status enc_bin_scratch_bytes(size_t nrays, const enc_bin_opts* bin, size_t* bytes);
+enc_status enc_intersect_closest_device_binned(enc_accel accel, const float* d_rays,
+                                               size_t nrays, enc_hit* d_hits, void* d_scratch,
+                                               size_t scratch_bytes, const enc_bin_opts* bin,
+                                               const enc_launch_opts* launch, enc_stream stream);
 
 /* Shadow / any-hit: occluded[i] = 1 iff some triangle is hit with
  * tmin < t < tmax.  This is the boolean PhotonMapperCPU::IsInShadow
@@ -231,10 +263,13 @@ enc_status enc_accel_count_visits(enc_accel accel, const float* d_rays, size_t n
  * enc_intersect_closest's.  Scratch (rays in, hits out, queue head, status)
  * is one fixed __device__ array inside this library, about 3 MiB per GPU that
  * loads it, held until exit; a batch may hold at most ENC_NOALLOC_MAX_RAYS
- * rays (more is ENC_ERR_INVALID_ARG).  The first call for a device looks up
- * the array's device address; make it before any stream capture.  Calls
- * share the array: calls from one process are serialised and synchronous,
- * and calls that overlap on the GPU race.  Wide-BVH accelerators only. */
+ * rays (more is ENC_ERR_INVALID_ARG).  enc_accel_build sets the array up on
+ * the accelerator's device (it looks up its device address, which makes the
+ * runtime create it, and runs this call's kernel once over an empty batch),
+ * so queries allocate nothing.  Calls share the array, which keeps the last
+ * call's contents; calls that overlapped on the GPU would race on it, so
+ * calls are serialised by a process-wide mutex and each returns only after
+ * its stream has drained.  Wide-BVH accelerators only. */
 #define ENC_NOALLOC_MAX_RAYS 65536
 enc_status enc_intersect_closest_noalloc(enc_accel accel, const float* rays, size_t nrays,
                                          enc_hit* hits, enc_stream stream);
@@ -276,11 +311,12 @@ typedef struct enc_server_s* enc_server;
 typedef struct enc_server_opts {
   int32_t device;
   uint32_t slots;          /* launches in flight at once (0 = 6) */
-  uint64_t slot_rays;      /* ray capacity of one slot; a request may not exceed it
-                              (0 = 4,194,304).  Smaller slots make more, smaller
-                              rounds whose copies overlap other rounds' traces:
-                              6 x 4M served 1.52x plain on a mixed 13M-ray pool,
-                              3 x 8M only 1.15x. */
+  uint64_t slot_rays;      /* ray capacity of one slot (0 = 4,194,304); a larger
+                              request is split into pieces of at most this many rays,
+                              traced over several rounds.  Smaller slots make more,
+                              smaller rounds whose copies overlap other rounds'
+                              traces: 6 x 4M served 1.52x plain on a mixed 13M-ray
+                              pool, 3 x 8M only 1.15x. */
   uint64_t budget_bytes;   /* HBM budget: resident scenes + slot buffers (0 = 120 GB) */
   enc_launch_opts launch;  /* kernel launch shape (zeros = defaults) */
 } enc_server_opts;
@@ -300,7 +336,10 @@ enc_status enc_server_create(const enc_server_opts* opts, enc_server* out);
 enc_status enc_server_add_scene(enc_server server, enc_accel accel, uint32_t* scene_id);
 /* Queues a request.  rays: host memory, 8 floats per ray (pinned memory lets
  * the copies overlap); out: host memory, enc_hit per ray (closest) or one
- * byte per ray (any); both must stay valid until the request completes. */
+ * byte per ray (any); both must stay valid until the request completes.  A
+ * request of more than slot_rays rays is split into slot-sized pieces; it is
+ * done when its last piece is.  Its status is its own: a kernel that stops
+ * at a loop bound on one piece fails only that piece's request. */
 enc_status enc_server_submit(enc_server server, uint32_t scene_id, int32_t kind,
                              const float* rays, uint64_t nrays, void* out, uint64_t* request_id);
 /* Waits up to timeout_s (< 0: forever) for a request; ENC_ERR_NOT_READY on
@@ -332,10 +371,12 @@ enc_status enc_camera_rays_device(const enc_camera* cam, float* d_rays, enc_stre
  * (TrianglePrim.cpp:236-239), 3 floats each per hit; NaN for misses. */
 enc_status enc_hit_surface_device(enc_accel accel, const enc_hit* d_hits, size_t n, float* d_pos,
                                   float* d_nrm, enc_stream stream);
-/* per_hit cosine-weighted diffuse rays from each closest hit, origin pushed
- * `offset` along the normal facing the incoming ray; output ray i*per_hit+k
- * belongs to hit i, misses give empty rays (tmax = 0).  Seeded, independent of
- * the launch shape. */
+/* per_hit cosine-weighted diffuse rays from each closest hit, drawn as
+ * randDirectionSuperN draws them (Common.cpp:144-182: cos^2(theta) uniform
+ * on [0.001, 1), azimuth uniform) about the geometric normal facing the
+ * incoming ray, origin pushed `offset` along that normal; output ray
+ * i*per_hit+k belongs to hit i, misses give empty rays (tmax = 0).  Seeded,
+ * independent of the launch shape. */
 enc_status enc_diffuse_rays_device(enc_accel accel, const float* d_rays, const enc_hit* d_hits,
                                    size_t n, uint32_t per_hit, uint32_t seed, float offset,
                                    float* d_out, enc_stream stream);
@@ -360,6 +401,39 @@ typedef struct enc_photon_opts {
 enc_status enc_photons_trace_device(enc_accel accel, const enc_photon_opts* opts, float* d_pos,
                                     float* d_nrm, float* d_pow, uint32_t capacity,
                                     uint32_t* stored, enc_stream stream);
+/* The reference's map split (PhotonMapperCPU.cpp:516-528, 701-745, 776-798):
+ * photons traced as enc_photons_trace_device traces them, each stored hit
+ * routed by ReflectPhotonDiffusely's rule -- the first hit of a path
+ * (bounce 0) into `direct`, later hits into `indirect` -- and, when
+ * shadow_offset > 0, a shadow photon for every bounce-0 hit: a ray from
+ * hitPoint + shadow_offset * dir along the same direction (the reference's
+ * offset is 2 at unit scale) that passes the surfaces it leaves (stepping
+ * emit_offset past each) and stores, at the first surface it enters, a photon
+ * with negative power and that surface's normal in `direct`.  There are no
+ * specular surfaces on this path, so no caustic map is filled.
+ *
+ * Photons are emitted in batches of opts->nphotons (path ids 0, 1, ...);
+ * with fill_indirect != 0, batches continue until `indirect` is full
+ * (EmitPhotons' while (!m_IndirectPhotonMap->Full()), :538-554), at most 64
+ * batches; otherwise one batch.  A full store drops further photons
+ * (PhotonMap::AddPhoton).  Every stored photon's power is then 1 / photons
+ * emitted (the light's unit power split evenly, as ScalePhotons scales it).
+ * d_tag (optional, may be NULL): per stored photon,
+ * path id << 4 | shadow << 3 | min(bounce, 7).  stored[0], stored[1]:
+ * photons in each store; *emitted (may be NULL): paths emitted.  Synchronises
+ * `stream`.  Paths of one call: at most 2^28. */
+typedef struct enc_photon_store {
+  float* d_pos;     /* 3 floats per photon */
+  float* d_nrm;     /* 3 floats per photon */
+  float* d_pow;     /* 3 floats per photon */
+  uint32_t* d_tag;  /* 1 word per photon, or NULL */
+  uint32_t capacity;
+} enc_photon_store;
+enc_status enc_photons_trace_maps_device(enc_accel accel, const enc_photon_opts* opts,
+                                         float shadow_offset, int32_t fill_indirect,
+                                         const enc_photon_store* direct,
+                                         const enc_photon_store* indirect, uint32_t stored[2],
+                                         uint32_t* emitted, enc_stream stream);
 /* PhotonMap over photon arrays in device memory (3 floats each per photon). */
 enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, const float* d_pow,
                                        size_t nphotons, int32_t caustic, int32_t device,
@@ -384,16 +458,33 @@ enum {
 /* GetRadianceEstimate (PhotonMap.cpp:121-164) for nq query points
  * (position + normal, 3 floats each); rgb gets 3 floats per query.
  * nq < 2^31 and k <= 256 (ENC_ERR_INVALID_ARG / ENC_ERR_UNSUPPORTED beyond).
- * The _device form is asynchronous on `stream`.  Calls on one map from
- * different streams may run at once: each launch takes its own work-queue
- * head, one of 256 per map, in turn. */
+ * The _device form is asynchronous on `stream` and does not read the
+ * kernel's status: call enc_photonmap_check after it.  Calls on one map from
+ * different streams may run at once: each launch takes the next of 256
+ * work-queue heads per map, in turn, so at most 256 launches on one map may
+ * be in flight together (the 257th would share the first one's head).  A
+ * launch captured into a CUDA graph keeps the head it was captured with;
+ * replays of it count against the same bound as eager launches. */
 enc_status enc_photonmap_radiance(enc_photonmap map, const float* qpos, const float* qnrm,
                                   size_t nq, int32_t k, float max_dist, int32_t flags,
                                   float* rgb, enc_stream stream);
+/* Waits for `stream` and reports ENC_ERR_WATCHDOG if any gather on this map
+ * stopped at its loop bound since the last check or synchronous call (the
+ * map's launches share one status word). */
+enc_status enc_photonmap_check(enc_photonmap map, enc_stream stream);
 enc_status enc_photonmap_radiance_device(enc_photonmap map, const float* d_qpos,
                                          const float* d_qnrm, size_t nq, int32_t k,
                                          float max_dist, int32_t flags, float* d_rgb,
                                          enc_stream stream);
+/* enc_photonmap_radiance_device that also writes, per query, the work
+ * behind the gather's bytes-per-query roofline into d_visits (4 words per
+ * query): child boxes tested (24 bytes each), photons tested (a 16-byte
+ * position each), normals read (16 bytes each), photons found (their 16-byte
+ * power).  Synchronises `stream`. */
+enc_status enc_photonmap_count_visits(enc_photonmap map, const float* d_qpos,
+                                      const float* d_qnrm, size_t nq, int32_t k, float max_dist,
+                                      int32_t flags, float* d_rgb, uint32_t* d_visits,
+                                      enc_stream stream);
 /* GetNearestNPhotons (PhotonMap.cpp:76-94): for each query the indices (into
  * the arrays given to enc_photonmap_create) and squared distances of the k
  * nearest accepted photons, ascending by distance, padded with -1; count[i]

@@ -41,11 +41,15 @@ def port():
         lib.eo_kd_build.argtypes = [P, C.c_int, P, P, P]
         lib.eo_kd_closest.argtypes = [P, P, C.c_long, C.c_int, P, C.c_int]
         lib.eo_kd_free.argtypes = [P]
+        lib.eo_kd_tested.argtypes = [P, P, P, C.c_long, C.c_int, P, C.c_int]
         lib.eo_pmap_build.restype = P
         lib.eo_pmap_build.argtypes = [P, P, P, C.c_long]
         lib.eo_pmap_gather.argtypes = [P, P, P, C.c_long, C.c_int, C.c_float, C.c_int, C.c_int,
                                        P, P, P, P, C.c_int]
         lib.eo_pmap_free.argtypes = [P]
+        lib.eo_photon_trace.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_float, C.c_int, P, P,
+                                        P, P, C.c_int]
+        lib.eo_photon_trace.restype = C.c_int
         _port = lib
     return _port
 
@@ -70,6 +74,9 @@ def reference():
         lib.encref_hardware_threads.restype = C.c_int
         lib.encref_model_load.restype = C.c_long
         lib.encref_model_load.argtypes = [C.c_char_p, P, C.c_float, C.c_float, P, P, C.c_long]
+        lib.encref_camera_rays.argtypes = [P, P, P, C.c_float, C.c_float, C.c_float, C.c_int,
+                                           C.c_int, P]
+        lib.encref_hit_surface.argtypes = [P, P, P, C.c_long, P, P]
         _ref = lib
     return _ref
 
@@ -133,32 +140,69 @@ def tri_test(tris, rays, ids, clamp=True):
     return acc.astype(bool), t, a, b
 
 
-def classify(tris, rays, got, want):
-    """Mismatch classes between two closest-hit results on the same rays:
-    'tie' (both triangles accepted by the FP32 predicate with the same t),
-    'want_false_positive' / 'got_false_positive' (that side's triangle is not
-    hit geometrically in FP64: a clamp artefact of the reference predicate),
-    'grazing' (|t_got - t_want| <= 1e-5 relative), 'unexplained'.
+def share_vertex(tris, a, b):
+    """True where triangles a[i] and b[i] (both >= 0) have a vertex with the
+    same three float coordinates (neighbours across an edge or a corner)."""
+    t = np.asarray(tris, np.float32).reshape(-1, 3, 3)
+    va = t[np.maximum(a, 0)][:, :, None, :]
+    vb = t[np.maximum(b, 0)][:, None, :, :]
+    same = np.all(va == vb, axis=-1).any(axis=(1, 2))
+    return same & (a >= 0) & (b >= 0)
+
+
+CLASS_NAMES = ("tie", "edge", "want_false_positive", "got_false_positive", "grazing",
+               "closer_untested", "unexplained")
+
+
+def classify(tris, rays, got, want, kd=None):
+    """Mismatch classes between two closest-hit results on the same rays
+    (got = the engine, want = the reference), first match wins:
+    'tie'   both triangles accepted by the FP32 predicate with the same t (a
+            shared edge met in a different order, H7);
+    'edge'  both accepted by the FP32 predicate, t within 1e-5 relative, and
+            the two triangles share a vertex: the ray crosses their common
+            edge or corner, and FP32 rounding decides which side accepts it;
+    'want_false_positive' / 'got_false_positive'  that side's triangle is not
+            hit geometrically in FP64 (a Cross() clamp artefact);
+    'grazing'  |t_got - t_want| <= 1e-5 relative, both geometric;
+    'closer_untested'  (only with kd = the reference's kd walk, a PortKd):
+            got's hit is geometric in FP64 and closer than want's (or want
+            misses), and the kd walk never tests got's triangle -- its cells
+            along the ray do not list it (a triangle that only touches a
+            cell's face is not distributed into it, Kdtree.cpp:579-585);
+    'unexplained'  anything else.
     Returns (indices of mismatches, list of class names)."""
     mism = np.nonzero(got["tri"] != want["tri"])[0]
     if len(mism) == 0:
         return mism, []
     r = rays[mism]
-    gh, gt = pairs_f64(tris, r, got["tri"][mism])
-    wh, wt = pairs_f64(tris, r, want["tri"][mism])
-    ga, gtt, _, _ = tri_test(tris, r, got["tri"][mism])
-    wa, wtt, _, _ = tri_test(tris, r, want["tri"][mism])
+    gid, wid = got["tri"][mism], want["tri"][mism]
+    gh, gt = pairs_f64(tris, r, gid)
+    wh, wt = pairs_f64(tris, r, wid)
+    ga, gtt, _, _ = tri_test(tris, r, gid)
+    wa, wtt, _, _ = tri_test(tris, r, wid)
+    nb = share_vertex(tris, gid, wid)
+    untested = np.zeros(len(mism), bool)
+    if kd is not None:
+        untested = ~kd.tested(r, gid)
     classes = []
     for j in range(len(mism)):
-        g_id, w_id = got["tri"][mism[j]], want["tri"][mism[j]]
+        g_id, w_id = gid[j], wid[j]
+        tg, tw = float(got["t"][mism[j]]), float(want["t"][mism[j]])
+        close = g_id >= 0 and w_id >= 0 and abs(tg - tw) <= 1e-5 * abs(tw)
         if g_id >= 0 and w_id >= 0 and ga[j] and wa[j] and gtt[j] == wtt[j]:
             classes.append("tie")
+        elif close and ga[j] and wa[j] and nb[j]:
+            classes.append("edge")
         elif w_id >= 0 and not wh[j]:
             classes.append("want_false_positive")
         elif g_id >= 0 and not gh[j]:
             classes.append("got_false_positive")
-        elif g_id >= 0 and w_id >= 0 and abs(float(got["t"][mism[j]]) - float(want["t"][mism[j]])) <= 1e-5 * abs(float(want["t"][mism[j]])):
+        elif close:
             classes.append("grazing")
+        elif (kd is not None and g_id >= 0 and gh[j] and (w_id < 0 or tg < tw)
+              and untested[j]):
+            classes.append("closer_untested")
         else:
             classes.append("unexplained")
     return mism, classes
@@ -179,6 +223,15 @@ class PortKd:
         self.lib.eo_kd_closest(self.h, rays.ctypes.data, rays.shape[0], int(clamp),
                                out.ctypes.data, nthreads)
         return out
+
+    def tested(self, rays, ids, clamp=True, nthreads=0):
+        """Per ray: does the reference kd walk test triangle ids[i] at all?"""
+        rays = _c(rays)
+        ids = _c(np.asarray(ids, dtype=np.int32))
+        out = np.zeros(rays.shape[0], np.uint8)
+        self.lib.eo_kd_tested(self.h, rays.ctypes.data, ids.ctypes.data, rays.shape[0],
+                              int(clamp), out.ctypes.data, nthreads)
+        return out.astype(bool)
 
     def __del__(self):
         try:
@@ -247,3 +300,72 @@ def ref_model_load(path, center, size, angle, axis):
     out = np.empty((n, 9), np.float32)
     lib.encref_model_load(b, c.ctypes.data, size, angle, ax.ctypes.data, out.ctypes.data, n)
     return out
+
+
+def ref_camera_rays(eye, look, up, fov_deg, width, height, near=1.0):
+    """Eye rays from the reference's own Camera basis and Vector3 arithmetic
+    (ref_harness.cpp:encref_camera_rays): (width*height, 8) float32."""
+    lib = reference()
+    e, l, u = (np.ascontiguousarray(x, np.float32) for x in (eye, look, up))
+    out = np.empty((width * height, 8), np.float32)
+    lib.encref_camera_rays(e.ctypes.data, l.ctypes.data, u.ctypes.data, float(fov_deg),
+                           float(np.float32(width / height)), float(near), int(width),
+                           int(height), out.ctypes.data)
+    return out
+
+
+def ref_hit_surface(tris, rays, ids):
+    """Hit point and normal that the reference's TrianglePrim::intersect stores
+    for ray i against triangle ids[i] (NaN where none): two (n, 3) arrays."""
+    lib = reference()
+    tris, rays = _c(np.asarray(tris, np.float32)), _c(np.asarray(rays, np.float32))
+    ids = _c(np.asarray(ids, dtype=np.int32))
+    n = len(ids)
+    pos = np.empty((n, 3), np.float32)
+    nrm = np.empty((n, 3), np.float32)
+    lib.encref_hit_surface(tris.ctypes.data, rays.ctypes.data, ids.ctypes.data, n,
+                           pos.ctypes.data, nrm.ctypes.data)
+    return pos, nrm
+
+
+class _PhotonOpts(C.Structure):
+    _fields_ = [("light_center", C.c_float * 3), ("light_size", C.c_float),
+                ("nphotons", C.c_uint32), ("max_bounces", C.c_uint32), ("albedo", C.c_float),
+                ("seed", C.c_uint32), ("emit_offset", C.c_float), ("bounce_offset", C.c_float)]
+
+
+class _PhotonOut(C.Structure):
+    _fields_ = [("pos", P), ("nrm", P), ("pow", P), ("tag", P), ("capacity", C.c_uint32)]
+
+
+def port_photon_trace(tris, light_center, light_size, nphotons, max_bounces=3, albedo=0.7,
+                      seed=1, emit_offset=0.01, bounce_offset=0.001, clamp=True, split=False,
+                      shadow_offset=0.0, fill=False, caps=(1 << 20, 1 << 20), nthreads=0):
+    """The oracle's photon tracer (encore_oracle.c:eo_photon_trace).  Returns a
+    list of one or two stores, each a dict of pos, nrm, pow (n, 3) and tag
+    (n,), plus the number of paths emitted."""
+    lib = port()
+    tris = _c(np.asarray(tris, np.float32))
+    o = _PhotonOpts((C.c_float * 3)(*light_center), light_size, nphotons, max_bounces, albedo,
+                    seed, emit_offset, bounce_offset)
+    stores, outs = [], []
+    for m in range(2 if split else 1):
+        cap = int(caps[m])
+        d = {"pos": np.zeros((cap, 3), np.float32), "nrm": np.zeros((cap, 3), np.float32),
+             "pow": np.zeros((cap, 3), np.float32), "tag": np.zeros(cap, np.uint32)}
+        stores.append(d)
+        outs.append(_PhotonOut(d["pos"].ctypes.data, d["nrm"].ctypes.data, d["pow"].ctypes.data,
+                               d["tag"].ctypes.data, cap))
+    stored = (C.c_uint32 * 2)()
+    emitted = C.c_uint32()
+    rc = lib.eo_photon_trace(tris.ctypes.data, tris.shape[0], C.byref(o), int(clamp), int(split),
+                             float(shadow_offset), int(fill), C.byref(outs[0]),
+                             C.byref(outs[1]) if split else None, stored, C.byref(emitted),
+                             nthreads)
+    if rc:
+        raise RuntimeError("oracle photon tracer: a shadow ray left 32 surfaces")
+    for m, d in enumerate(stores):
+        k = stored[m]
+        for key in d:
+            d[key] = d[key][:k]
+    return stores, emitted.value

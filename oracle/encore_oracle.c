@@ -440,6 +440,8 @@ typedef struct {
   const float* rays;
   int clamp;
   eo_hit* out;
+  const int32_t* probe; /* optional: per ray, a triangle ID to watch for */
+  uint8_t* tested;      /* with probe: 1 if the walk tested that triangle */
 } kd_ctx;
 
 /* Kdtree::intersect (Kdtree.cpp:682-784). */
@@ -455,6 +457,8 @@ static void kd_closest_range(void* p, long b, long e) {
     const float inv[3] = {1.f / d[0], 1.f / d[1], 1.f / d[2]};
     float best = INFINITY, ba = 0.f, bb = 0.f;
     int best_id = -1;
+    const int32_t watch = c->probe ? c->probe[i] : -1;
+    if (c->tested) c->tested[i] = 0;
     /* AABB::Intersect(Ray&, float&, float&) (AABB.cpp:117-143) */
     float t0 = 0, t1 = INFINITY;
     int in = 1;
@@ -506,6 +510,7 @@ static void kd_closest_range(void* p, long b, long e) {
           uint32_t cnt = nd.w0 >> 2;
           for (uint32_t k = 0; k < cnt; ++k) {
             uint32_t id = kd->items[nd.w1 + k];
+            if (watch >= 0 && (int32_t)id == watch) c->tested[i] = 1;
             float t, a, bt;
             if (eo_tri_test(kd->tris + 9 * (size_t)id, r, c->clamp, &t, &a, &bt) && t < best) {
               best = t;
@@ -537,8 +542,16 @@ static void kd_closest_range(void* p, long b, long e) {
 }
 
 void eo_kd_closest(void* kd, const float* rays, long n, int clamp, eo_hit* out, int nthreads) {
-  kd_ctx c = {(kdtree*)kd, rays, clamp, out};
+  kd_ctx c = {(kdtree*)kd, rays, clamp, out, NULL, NULL};
   parallel_range(n, nthreads, kd_closest_range, &c);
+}
+
+void eo_kd_tested(void* kd, const float* rays, const int32_t* ids, long n, int clamp,
+                  uint8_t* tested, int nthreads) {
+  eo_hit* out = (eo_hit*)malloc((size_t)(n > 0 ? n : 1) * sizeof(eo_hit));
+  kd_ctx c = {(kdtree*)kd, rays, clamp, out, ids, tested};
+  parallel_range(n, nthreads, kd_closest_range, &c);
+  free(out);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -786,4 +799,266 @@ void eo_pmap_gather(void* pm, const float* qpos, const float* qnrm, long nq, int
   gather_ctx c = {(const pmap*)pm, qpos, qnrm, k, max_dist, ignore_normal, caustic,
                   rgb, idx, d2, count};
   parallel_range(nq, nthreads, gather_range, &c);
+}
+
+/* ------------------------------------------------------------------------ */
+/* f1: photon tracing (the device tracer's algorithm, restated)              */
+/*                                                                           */
+/* The engine traces photons as PhotonMapperCPU::EmitPhotons / TracePhoton / */
+/* ReflectPhotonDiffusely / EmitShadowPhoton do (PhotonMapperCPU.cpp:503-798) */
+/* with its own seeded counter-based random numbers (the reference's rand()  */
+/* is not reproducible, H12).  This is that algorithm written out path by    */
+/* path in plain C, with the oracle's brute-force closest hit: given the    */
+/* same closest hits it produces the same photons bit for bit.               */
+
+static uint32_t ph_hash32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+static float ph_rnd(uint32_t seed, uint32_t path, uint32_t draw) {
+  const uint32_t h = ph_hash32(seed ^ ph_hash32(path * 0x9E3779B9u ^ ph_hash32(draw + 0x632BE5ABu)));
+  return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
+/* Vector3::Normalize (Vector3.cpp:105-124): divide by sqrt((x*x + y*y) + z*z),
+ * then ClampfloatoZero each component. */
+static void ph_normalize(float* v) {
+  const float m = sqrtf((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+  for (int i = 0; i < 3; ++i) v[i] = clamp_eps(v[i] / m);
+}
+
+/* The cut cosine lobe about n: cos^2(theta) uniform on [lo, 1) from a point
+ * on the unit disk drawn by rejection (16 tries, draws draw0 + 2j, + 1),
+ * scaled by sqrt(1 - lo); frame t = normalize(a' x n), b = n x t. */
+static void ph_lobe(const float* n_in, float lo, uint32_t seed, uint32_t path, uint32_t draw0,
+                    float* d) {
+  float n[3] = {n_in[0], n_in[1], n_in[2]};
+  ph_normalize(n);
+  const float R = sqrtf(1.0f - lo);
+  float x = 0.f, y = 0.f, r2 = 0.f;
+  for (int j = 0; j < 16; ++j) {
+    const float a = 2.0f * ph_rnd(seed, path, draw0 + 2 * j) - 1.0f;
+    const float b = 2.0f * ph_rnd(seed, path, draw0 + 2 * j + 1) - 1.0f;
+    if (a * a + b * b <= 1.0f) {
+      x = a * R;
+      y = b * R;
+      r2 = x * x + y * y;
+      break;
+    }
+  }
+  const float z = sqrtf(1.0f - r2);
+  float t[3];
+  if (fabsf(n[0]) > 0.9f) {
+    t[0] = n[2];
+    t[1] = 0.0f;
+    t[2] = -n[0];
+  } else {
+    t[0] = 0.0f;
+    t[1] = -n[2];
+    t[2] = n[1];
+  }
+  const float tl = sqrtf((t[0] * t[0] + t[1] * t[1]) + t[2] * t[2]);
+  for (int i = 0; i < 3; ++i) t[i] = t[i] / tl;
+  const float b[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2],
+                      n[0] * t[1] - n[1] * t[0]};
+  for (int i = 0; i < 3; ++i) d[i] = (x * t[i] + y * b[i]) + z * n[i];
+  ph_normalize(d);
+}
+
+typedef struct {
+  const float* tris;
+  int ntris;
+  int clamp;
+} ph_scene;
+
+/* Closest hit: the lowest t, then the lowest ID (BasicAS order). */
+static int ph_closest(const ph_scene* S, const float* r, float* a, float* b) {
+  int id = -1;
+  float best = r[7];
+  for (int k = 0; k < S->ntris; ++k) {
+    float t, aa, bb;
+    if (eo_tri_test(S->tris + 9 * (size_t)k, r, S->clamp, &t, &aa, &bb) && t < best) {
+      best = t;
+      id = k;
+      *a = aa;
+      *b = bb;
+    }
+  }
+  return id;
+}
+
+/* TrianglePrim::intersect's hit point and stored normal. */
+static void ph_surface(const float* tri, float a, float b, float* p, float* n) {
+  const float e1[3] = {tri[3] - tri[0], tri[4] - tri[1], tri[5] - tri[2]};
+  const float e2[3] = {tri[6] - tri[0], tri[7] - tri[1], tri[8] - tri[2]};
+  for (int i = 0; i < 3; ++i) p[i] = (tri[i] + e1[i] * a) + e2[i] * b;
+  cross_ref(e1, e2, 1, n);
+  ph_normalize(n);
+}
+
+typedef struct {
+  float pos[3], nrm[3], power;
+  uint32_t tag;
+  int store;
+} ph_photon;
+
+typedef struct {
+  ph_scene S;
+  eo_photon_opts o;
+  uint32_t path0;
+  int split;
+  float shadow_offset;
+  int max_per_path;
+  ph_photon* out; /* max_per_path per path */
+  int* count;     /* per path */
+  long shadow_dropped;
+} ph_ctx;
+
+static void ph_ray(float* r, const float* o, const float* d) {
+  r[0] = o[0];
+  r[1] = o[1];
+  r[2] = o[2];
+  r[3] = 0.0f;
+  r[4] = d[0];
+  r[5] = d[1];
+  r[6] = d[2];
+  r[7] = INFINITY;
+}
+
+static void ph_trace_range(void* p, long b, long e) {
+  ph_ctx* c = (ph_ctx*)p;
+  const eo_photon_opts* o = &c->o;
+  const uint32_t seed = o->seed ? o->seed : 1u;
+  for (long i = b; i < e; ++i) {
+    const uint32_t id = c->path0 + (uint32_t)i;
+    ph_photon* out = c->out + (size_t)i * c->max_per_path;
+    int k = 0;
+    /* RectangleLight::EmitPhoton + TracePhoton's first ray */
+    const float lp[3] = {o->light_center[0] + (ph_rnd(seed, id, 0) - 0.5f) * o->light_size,
+                         o->light_center[1],
+                         o->light_center[2] + (ph_rnd(seed, id, 1) - 0.5f) * o->light_size};
+    const float down[3] = {0.f, -1.f, 0.f};
+    float d[3];
+    ph_lobe(down, 0.01f, seed, id, 2, d);
+    float org[3] = {lp[0] + d[0] * o->emit_offset, lp[1] + d[1] * o->emit_offset,
+                    lp[2] + d[2] * o->emit_offset};
+    float r[8];
+    ph_ray(r, org, d);
+    for (uint32_t wave = 0; wave <= o->max_bounces; ++wave) {
+      float a, bb;
+      const int hid = ph_closest(&c->S, r, &a, &bb);
+      if (hid < 0) break;
+      const float* tri = c->S.tris + 9 * (size_t)hid;
+      float hp[3], hn[3];
+      ph_surface(tri, a, bb, hp, hn);
+      ph_photon* ph = &out[k++];
+      memcpy(ph->pos, hp, sizeof hp);
+      memcpy(ph->nrm, hn, sizeof hn);
+      ph->power = 1.0f;
+      ph->tag = (id << 4) | (wave < 7 ? wave : 7u);
+      ph->store = (c->split && wave > 0) ? 1 : 0;
+      if (wave == 0 && c->shadow_offset > 0.0f) {
+        /* EmitShadowPhoton: from hitPoint + dir * shadow_offset on */
+        const float* sd = r + 4;
+        float so[3] = {hp[0] + sd[0] * c->shadow_offset, hp[1] + sd[1] * c->shadow_offset,
+                       hp[2] + sd[2] * c->shadow_offset};
+        float sr[8];
+        ph_ray(sr, so, sd);
+        for (int step = 0; step < 32; ++step) {
+          float sa, sb;
+          const int sid = ph_closest(&c->S, sr, &sa, &sb);
+          if (sid < 0) break;
+          float sp[3], sn[3];
+          ph_surface(c->S.tris + 9 * (size_t)sid, sa, sb, sp, sn);
+          const float dn = (sd[0] * sn[0] + sd[1] * sn[1]) + sd[2] * sn[2];
+          if (dn < 0.0f) {
+            ph_photon* q = &out[k++];
+            memcpy(q->pos, sp, sizeof sp);
+            memcpy(q->nrm, sn, sizeof sn);
+            q->power = -1.0f;
+            q->tag = (id << 4) | 8u;
+            q->store = 0;
+            break;
+          }
+          if (step == 31) {
+            __atomic_fetch_add(&c->shadow_dropped, 1, __ATOMIC_RELAXED);
+            break;
+          }
+          so[0] = sp[0] + sd[0] * o->emit_offset;
+          so[1] = sp[1] + sd[1] * o->emit_offset;
+          so[2] = sp[2] + sd[2] * o->emit_offset;
+          ph_ray(sr, so, sd);
+        }
+      }
+      if (wave >= o->max_bounces) break;
+      if (!(ph_rnd(seed, id, 64u + 64u * wave) < o->albedo)) break;
+      float nd[3];
+      ph_lobe(hn, 0.001f, seed, id, 65u + 64u * wave, nd);
+      if (!(nd[0] == nd[0]) || !(nd[1] == nd[1]) || !(nd[2] == nd[2])) break;
+      const float no[3] = {hp[0] + nd[0] * o->bounce_offset, hp[1] + nd[1] * o->bounce_offset,
+                           hp[2] + nd[2] * o->bounce_offset};
+      ph_ray(r, no, nd);
+    }
+    c->count[i] = k;
+  }
+}
+
+int eo_photon_trace(const float* tris, int ntris, const eo_photon_opts* o, int clamp, int split,
+                    float shadow_offset, int fill, eo_photon_out* s0, eo_photon_out* s1,
+                    uint32_t* stored, uint32_t* emitted, int nthreads) {
+  ph_ctx c;
+  memset(&c, 0, sizeof c);
+  c.S.tris = tris;
+  c.S.ntris = ntris;
+  c.S.clamp = clamp;
+  c.o = *o;
+  c.split = split;
+  c.shadow_offset = shadow_offset;
+  c.max_per_path = (int)o->max_bounces + 2;
+  const long n = o->nphotons;
+  uint64_t offered[2] = {0, 0};
+  stored[0] = stored[1] = 0;
+  uint32_t batches = 0;
+  uint64_t total = 0;
+  if (n == 0) {
+    if (emitted) *emitted = 0;
+    return 0;
+  }
+  c.out = (ph_photon*)malloc((size_t)n * c.max_per_path * sizeof(ph_photon));
+  c.count = (int*)malloc((size_t)n * sizeof(int));
+  eo_photon_out* st[2] = {s0, s1};
+  for (;;) {
+    c.path0 = (uint32_t)total;
+    parallel_range(n, nthreads, ph_trace_range, &c);
+    for (long i = 0; i < n; ++i) {
+      for (int k = 0; k < c.count[i]; ++k) {
+        const ph_photon* ph = &c.out[(size_t)i * c.max_per_path + k];
+        const int m = ph->store;
+        const uint64_t slot = offered[m]++;
+        if (!st[m] || slot >= st[m]->capacity) continue;
+        memcpy(st[m]->pos + 3 * slot, ph->pos, 3 * sizeof(float));
+        memcpy(st[m]->nrm + 3 * slot, ph->nrm, 3 * sizeof(float));
+        for (int q = 0; q < 3; ++q) st[m]->pow[3 * slot + q] = ph->power;
+        if (st[m]->tag) st[m]->tag[slot] = ph->tag;
+      }
+    }
+    total += (uint64_t)n;
+    ++batches;
+    if (!fill || !s1 || offered[1] >= s1->capacity || batches >= 64) break;
+  }
+  const float scale = (float)(1.0 / (double)total);
+  for (int m = 0; m < 2; ++m) {
+    if (!st[m]) continue;
+    stored[m] = (uint32_t)(offered[m] < st[m]->capacity ? offered[m] : st[m]->capacity);
+    for (uint64_t j = 0; j < 3ull * stored[m]; ++j) st[m]->pow[j] = st[m]->pow[j] * scale;
+  }
+  if (emitted) *emitted = (uint32_t)total;
+  free(c.out);
+  free(c.count);
+  return c.shadow_dropped ? 1 : 0;
 }

@@ -58,6 +58,10 @@ void eo_pairs_f64(const float* tris, const float* rays, const int32_t* ids, long
 void* eo_kd_build(const float* tris, int ntris, int* max_depth, long* nnodes, long* nitems);
 void eo_kd_closest(void* kd, const float* rays, long n, int clamp, eo_hit* out, int nthreads);
 void eo_kd_free(void* kd);
+/* The same walk, reporting per ray whether it tested triangle ids[i] at all
+ * (ids[i] < 0: never).  Used to explain a closer hit the walk passed over. */
+void eo_kd_tested(void* kd, const float* rays, const int32_t* ids, long n, int clamp,
+                  uint8_t* tested, int nthreads);
 
 /* Photon gather: the k nearest accepted photons within max_dist
  * (PhotonMap::GetNearestNPhotons, PhotonMap.cpp:76-94, 224-297: accept
@@ -70,6 +74,35 @@ void eo_pmap_gather(void* pm, const float* qpos, const float* qnrm, long nq, int
                     float max_dist, int ignore_normal, int caustic, double* rgb, int32_t* idx,
                     float* d2, int32_t* count, int nthreads);
 void eo_pmap_free(void* pm);
+
+/* Photon tracing as the engine traces photons (enc_photons_trace_device /
+ * _maps_device; PhotonMapperCPU.cpp:503-798 with the engine's seeded random
+ * numbers), path by path, with the brute-force closest hit (clamp selects
+ * the reference predicate).  split: bounce 0 -> s0 (direct), later -> s1
+ * (indirect); else all -> s0.  shadow_offset > 0: shadow photons into s0.
+ * fill: batches of opts->nphotons until s1 is full (at most 64).  Photons
+ * past a store's capacity are dropped in path order.  Powers: 1/emitted, the
+ * shadow photons' negative.  Returns 1 if a shadow ray left 32 surfaces. */
+typedef struct eo_photon_opts {
+  float light_center[3];
+  float light_size;
+  uint32_t nphotons;
+  uint32_t max_bounces;
+  float albedo;
+  uint32_t seed;
+  float emit_offset;
+  float bounce_offset;
+} eo_photon_opts;
+typedef struct eo_photon_out {
+  float* pos;
+  float* nrm;
+  float* pow;
+  uint32_t* tag; /* may be NULL */
+  uint32_t capacity;
+} eo_photon_out;
+int eo_photon_trace(const float* tris, int ntris, const eo_photon_opts* o, int clamp, int split,
+                    float shadow_offset, int fill, eo_photon_out* s0, eo_photon_out* s1,
+                    uint32_t* stored, uint32_t* emitted, int nthreads);
 
 #ifdef __cplusplus
 }

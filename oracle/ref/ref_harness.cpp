@@ -13,6 +13,8 @@
 //   PhotonMap::GetNearestNPhotons       ENCORE/src/renderers/PhotonMap.cpp:76-94, 224-297
 //   PhotonMap::GetRadianceEstimate      ENCORE/src/renderers/PhotonMap.cpp:121-164
 //   PhotonMapperCPU::IsInShadow         ENCORE/src/renderers/PhotonMapperCPU.cpp:1192-1207
+//   Camera::Camera / CalcCamVectors     ENCORE/src/scene/Camera.cpp:12-18, 85-93, 157-166
+//   TrianglePrim::intersect's hit point and normal  TrianglePrim.cpp:236-239
 //
 // It is the checker used by tests and the timed CPU arm of bench.py; nothing
 // in the engine links it.
@@ -36,6 +38,9 @@
 #include "Color.h"
 #include "Model.h"
 #include "Material.h"
+#include "Camera.h"
+#include "Common.h"
+#include "Ray.h"
 
 extern bool IGNORE_NORMAL;  // ENCORE/src/renderers/PhotonMap.cpp:23
 
@@ -296,6 +301,79 @@ long encref_model_load(const char* path, const float* center, float size, float 
     delete ts;
   }
   return (long)pl.size();
+}
+
+
+// Eye rays of RayTracer::CalcEyeRaySamples (RayTracer.cpp:489-525) for one
+// unjittered sample per pixel (m_BlockSize = 1, so x = col + 0.5), row-major
+// from the bottom row.  The camera basis is the reference's own Camera (the
+// three-argument constructor, which keeps `up`; Camera::set ignores its `up`
+// argument, Camera.cpp:44) with SetViewVolume's view angle, aspect and near
+// plane, and all vector arithmetic is the reference's Vector3.  The loop body
+// is the expression of RayTracer.cpp:495-516 written out here, because
+// RayTracer.cpp itself needs the renderer's GL classes.  out: 8 floats per ray
+// (eye, 0, direction, +inf).
+void encref_camera_rays(const float* eye, const float* look, const float* up, float fov_deg,
+                        float aspect, float near_plane, int width, int height, float* out) {
+  Camera cam(Point3(eye[0], eye[1], eye[2]), Point3(look[0], look[1], look[2]),
+             Vector3(up[0], up[1], up[2]));
+  cam.SetViewVolume(fov_deg, aspect, near_plane, 1000.0f);
+  const int block = 1;
+  float H = cam.GetNearClipPlane() * tan(cam.GetViewAngle() * (PI / 360.0));
+  float W = H * cam.GetAspect();
+  for (int row = 0; row < height; ++row) {
+    for (int col = 0; col < width; ++col) {
+      float x = col + (block / 2.0f);
+      float y = row + (block / 2.0f);
+      float Uc = -W + (W * (2 * x) / (float)width);
+      float Vr = -H + (H * (2 * y) / (float)height);
+      float N = cam.GetNearClipPlane();
+      Vector3 n = cam.N() * -N;
+      Vector3 u = cam.U() * Uc;
+      Vector3 v = cam.V() * Vr;
+      Vector3 direction = n + u + v;
+      direction.Normalize();
+      Point3 e = cam.GetEye();
+      float* o = out + 8 * ((size_t)row * width + col);
+      o[0] = e.X();
+      o[1] = e.Y();
+      o[2] = e.Z();
+      o[3] = 0.0f;
+      o[4] = direction.X();
+      o[5] = direction.Y();
+      o[6] = direction.Z();
+      o[7] = INFINITY;
+    }
+  }
+}
+
+// The hit point and normal TrianglePrim::intersect stores for ray i against
+// triangle ids[i] (TrianglePrim.cpp:236-239), computed by the reference's
+// own intersect on that one triangle; NaN where ids[i] < 0 or the reference
+// reports no hit.  rays: 8 floats each (origin, tmin, direction, tmax).
+void encref_hit_surface(const float* tri_verts, const float* rays, const int* ids, long n,
+                        float* pos, float* nrm) {
+  const float qnan = NAN;
+  for (long i = 0; i < n; ++i) {
+    float* p = pos + 3 * i;
+    float* q = nrm + 3 * i;
+    p[0] = p[1] = p[2] = q[0] = q[1] = q[2] = qnan;
+    if (ids[i] < 0) continue;
+    const float* c = tri_verts + 9 * (size_t)ids[i];
+    Vertex v0(c[0], c[1], c[2], 0.f, 0.f, 1.f), v1(c[3], c[4], c[5], 0.f, 0.f, 1.f),
+        v2(c[6], c[7], c[8], 0.f, 0.f, 1.f);
+    TrianglePrim prim(v0, v1, v2);
+    const float* r = rays + 8 * i;
+    Ray ray(Point3(r[0], r[1], r[2]), Vector3(r[4], r[5], r[6]));
+    HitInfo hit;
+    if (!prim.intersect(ray, &hit)) continue;
+    p[0] = hit.hitPoint.X();
+    p[1] = hit.hitPoint.Y();
+    p[2] = hit.hitPoint.Z();
+    q[0] = hit.hitNormal.X();
+    q[1] = hit.hitNormal.Y();
+    q[2] = hit.hitNormal.Z();
+  }
 }
 
 }  // extern "C"

@@ -117,11 +117,45 @@ def photon_fixture(scale: float, ignore_normal: bool) -> None:
     print(name, "mean count", float(out["count_c0"].mean()))
 
 
+CAMERAS = [
+    # eye, look, up, vertical fov, width, height
+    ((0.5, 0.5, -1.5), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), 45.0, 64, 48),
+    ((500.0, 1300.0, 500.0), (500.0, 0.0, 500.0), (0.0, 0.0, 1.0), 40.0, 33, 65),
+    ((500.0, 500.0, -1500.0), (500.0, 500.0, 500.0), (0.0, 1.0, 0.0), 45.0, 128, 128),
+    ((-2.0, 3.0, 4.0), (0.25, 0.0, -0.5), (0.3, 1.0, 0.1), 60.0, 40, 30),
+]
+
+
+def camera_surface_fixture() -> None:
+    """Eye rays from the reference's Camera basis and Vector3 arithmetic
+    (the formula of RayTracer::CalcEyeRaySamples), and the hit point and
+    normal the reference's TrianglePrim::intersect stores for the Kdtree's
+    hits on the random2k x1000 scene."""
+    out = {}
+    for i, (eye, look, up, fov, w, h) in enumerate(CAMERAS):
+        out[f"cam{i}_params"] = np.array([*eye, *look, *up, fov, w, h], np.float64)
+        out[f"cam{i}_rays"] = ob.ref_camera_rays(eye, look, up, fov, w, h)
+    g = np.load(OUT / "random2k_x1000.npz")
+    tris, rays, ids = g["tris"], g["rays"], g["kd_tri"]
+    pos, nrm = ob.ref_hit_surface(tris, rays, ids)
+    out.update(ncams=np.int32(len(CAMERAS)), surf_ids=ids, surf_pos=pos, surf_nrm=nrm)
+    np.savez_compressed(OUT / "camera_surface.npz", **out)
+    print("camera_surface.npz", len(CAMERAS), "cameras,", int((ids >= 0).sum()), "surfaces")
+
+
+FIXTURES = {
+    "random2k_x1": lambda: random_scene_fixture(1.0),
+    "random2k_x1000": lambda: random_scene_fixture(1000.0),
+    "heightfield64_x1000": heightfield_fixture,
+    "photons20k_x1_ignore": lambda: photon_fixture(1.0, ignore_normal=True),
+    "photons20k_x1000_normal": lambda: photon_fixture(1000.0, ignore_normal=False),
+    "camera_surface": camera_surface_fixture,
+}
+
+
 if __name__ == "__main__":
+    # python tests/golden/make_golden.py [fixture ...]   (no names: all of them)
     if ob.reference() is None:
         sys.exit("oracle/_ref/libencore_ref.so missing: run `make -C oracle ref` first")
-    random_scene_fixture(1.0)
-    random_scene_fixture(1000.0)
-    heightfield_fixture()
-    photon_fixture(1.0, ignore_normal=True)
-    photon_fixture(1000.0, ignore_normal=False)
+    for name in (sys.argv[1:] or list(FIXTURES)):
+        FIXTURES[name]()

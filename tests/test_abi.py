@@ -10,7 +10,7 @@ HEADER = Path(__file__).resolve().parents[1] / "include" / "encore_b200.h"
 
 def declared_symbols():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:enc_status|int32_t|const char\*)\s+(enc_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:enc_status|int32_t|double|const char\*)\s+(enc_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_entry_points():

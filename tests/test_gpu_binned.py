@@ -1,0 +1,97 @@
+"""Binned closest hit (enc_intersect_closest_device_binned, GPU): the batch is
+counting-sorted by a key of origin cell and direction cell before the
+traversal, and the hits must be the unbinned launch's bit for bit -- binning
+changes only which rays share a warp, never a ray's result -- and both must
+match the oracle."""
+import numpy as np
+import pytest
+
+from encore_b200 import Accelerator, BinConfig, EncoreError, scenes
+from oracle import bindings as ob
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev_hits(acc, rays, binning=None, device=0):
+    import torch
+    n = len(rays)
+    d_rays = torch.from_numpy(np.ascontiguousarray(rays)).to(device)
+    d_plain = torch.full((max(n, 1), 4), -7, dtype=torch.int32, device=device)
+    d_bin = torch.full((max(n, 1), 4), -9, dtype=torch.int32, device=device)
+    acc.intersect_device(d_rays, n, d_plain)
+    scratch = torch.empty(acc.bin_scratch_bytes(n, binning), dtype=torch.uint8, device=device)
+    acc.intersect_device_binned(d_rays, n, d_bin, scratch, binning)
+    acc.check()
+    return d_plain[:n].cpu().numpy(), d_bin[:n].cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def field():
+    tris = scenes.heightfield(res=128, seed=3, scale=1000.0)
+    acc = Accelerator("wbvh").build(tris)
+    prim = scenes.camera_rays(128, 128, eye=np.array([0.5, 1.3, 0.5]) * 1000.0,
+                              look=np.array([0.5, 0.0, 0.5]) * 1000.0, up=(0.0, 0.0, 1.0),
+                              fov_deg=40.0)
+    ph = acc.intersect(prim)
+    sec = scenes.diffuse_rays(tris, prim, ph["tri"], ph["u"], ph["v"], per_hit=3, seed=4,
+                              offset=0.1)
+    rays = np.concatenate([prim, sec])
+    rays = np.ascontiguousarray(rays[np.random.default_rng(5).permutation(len(rays))])
+    return tris, rays, acc
+
+
+@pytest.mark.parametrize("cfg", [None, BinConfig(10, 6), BinConfig(16, 0), BinConfig(0, 12),
+                                 BinConfig(1, 0), BinConfig(12, 8), BinConfig(12, 0, 0.05),
+                                 BinConfig(9, 9, 0.2)])
+def test_binned_equals_plain_and_oracle(gpu, field, cfg):
+    tris, rays, acc = field
+    plain, binned = _dev_hits(acc, rays, cfg)
+    assert np.array_equal(plain, binned)
+    sub = np.arange(0, len(rays), 7)
+    want = ob.port_brute(tris, rays[sub], clamp=True)
+    got = binned[sub]
+    mism, classes = ob.classify(tris, rays[sub], got.view(ob.HIT).reshape(-1), want)
+    assert set(classes) <= {"tie"}, classes
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 1000, 4097])
+def test_binned_ragged_sizes(gpu, field, n):
+    tris, rays, acc = field
+    plain, binned = _dev_hits(acc, rays[:n])
+    assert np.array_equal(plain, binned)
+
+
+def test_binned_random_triangles_unit_scale(gpu):
+    """The CPU-runnable plain case at unit scale (clamp artefacts included):
+    binning must not change a single result."""
+    tris = scenes.random_triangles(10000, seed=0, scale=1.0)
+    rays = scenes.camera_rays(256, 256, eye=np.array([0.5, 0.5, -1.5]),
+                              look=np.array([0.5, 0.5, 0.5]))
+    sph = scenes.random_sphere_rays(20000, seed=9)
+    rays = np.concatenate([rays, sph])
+    acc = Accelerator("wbvh").build(tris)
+    plain, binned = _dev_hits(acc, rays, BinConfig(8, 8))
+    assert np.array_equal(plain, binned)
+    acc.destroy()
+
+
+def test_binned_argument_errors(gpu, field):
+    import torch
+    tris, rays, acc = field
+    n = 1000
+    d_rays = torch.from_numpy(rays[:n]).to(0)
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device=0)
+    need = acc.bin_scratch_bytes(n)
+    small = torch.empty(need - 256, dtype=torch.uint8, device=0)
+    with pytest.raises(EncoreError):
+        acc.intersect_device_binned(d_rays, n, d_hits, small)
+    big = torch.empty(need + 256, dtype=torch.uint8, device=0)
+    with pytest.raises(EncoreError):  # not 256-byte aligned
+        acc.intersect_device_binned(d_rays, n, d_hits, big[16:])
+    with pytest.raises(EncoreError):  # more than 20 key bits
+        acc.bin_scratch_bytes(n, BinConfig(16, 8))
+    kd = Accelerator("kdtree").build(tris[:200])
+    with pytest.raises(EncoreError):
+        kd.intersect_device_binned(d_rays, n, d_hits, big)
+    kd.destroy()
+    acc.intersect_device_binned(d_rays, 0, d_hits, big)  # empty batch: nothing to do

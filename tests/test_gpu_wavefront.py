@@ -1,8 +1,9 @@
 """Device-side ray and photon generation (GPU): eye rays bit-exact with the
-host restatement of RayTracer::CalcEyeRaySamples, hit surfaces bit-exact
-with TrianglePrim::intersect's hit point and normal, diffuse rays and photon
-paths well formed and reproducible, and the photon-map pipeline's radiance
-within 1e-4 of the FP64 oracle."""
+reference's own camera (RayTracer::CalcEyeRaySamples over Camera's basis),
+hit surfaces bit-exact with what the reference's TrianglePrim::intersect
+stores, diffuse rays with randDirectionSuperN's distribution, photon paths
+well formed and reproducible, and the photon-map pipeline's radiance within
+1e-4 of the FP64 oracle."""
 import numpy as np
 import pytest
 
@@ -22,46 +23,94 @@ def bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.int32)
 
 
-@pytest.mark.parametrize("cam", [
-    dict(eye=(500.0, 500.0, -1500.0), look=(500.0, 500.0, 500.0), up=(0.0, 1.0, 0.0), fov=45.0, w=64, h=48),
-    dict(eye=(500.0, 1300.0, 500.0), look=(500.0, 0.0, 500.0), up=(0.0, 0.0, 1.0), fov=40.0, w=33, h=65),
-    dict(eye=(0.5, 0.5, -1.5), look=(0.5, 0.5, 0.5), up=(0.0, 1.0, 0.0), fov=45.0, w=128, h=128),
-])
-def test_camera_rays_bit_exact_with_host_restatement(gpu, cam):
+GOLD = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def _camera_cases():
+    g = np.load(GOLD / "camera_surface.npz")
+    return [(g[f"cam{i}_params"], g[f"cam{i}_rays"]) for i in range(int(g["ncams"]))]
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_camera_rays_bit_exact_with_reference(gpu, case):
+    """camera_kernel against eye rays that the reference's own Camera basis and
+    Vector3 arithmetic produced (tests/golden/camera_surface.npz, made by
+    tests/golden/make_golden.py from the compiled reference)."""
     import torch
-    want = scenes.camera_rays(cam["w"], cam["h"], eye=cam["eye"], look=cam["look"], up=cam["up"],
-                              fov_deg=cam["fov"])
-    d = torch.empty((cam["w"] * cam["h"], 8), dtype=torch.float32, device="cuda")
-    wavefront.camera_rays(cam["eye"], cam["look"], cam["up"], cam["fov"], cam["w"], cam["h"], d)
+    p, want = _camera_cases()[case]
+    eye, look, up, fov, w, h = tuple(p[0:3]), tuple(p[3:6]), tuple(p[6:9]), float(p[9]), int(p[10]), int(p[11])
+    d = torch.empty((w * h, 8), dtype=torch.float32, device="cuda")
+    wavefront.camera_rays(eye, look, up, fov, w, h, d)
     torch.cuda.synchronize()
     got = d.cpu().numpy()
     assert np.array_equal(bits(got[:, :7]), bits(want[:, :7]))
     assert np.all(np.isinf(got[:, 7]))
 
 
-def test_hit_surface_bit_exact(gpu):
+def test_hit_surface_bit_exact_with_reference(gpu):
+    """surface_kernel on the reference Kdtree's hits (random2k x1000 golden)
+    against the hit point and normal the reference's TrianglePrim::intersect
+    stored for them."""
     import torch
-    tris = scenes.random_triangles(8000, seed=61, scale=SCALE)
-    rays = scenes.camera_rays(96, 96, eye=np.array([0.5, 0.5, -1.5]) * SCALE,
-                              look=np.array([0.5, 0.5, 0.5]) * SCALE)
+    g = np.load(GOLD / "random2k_x1000.npz")
+    s = np.load(GOLD / "camera_surface.npz")
+    tris = g["tris"]
+    n = len(g["rays"])
+    hits = np.zeros(n, ob.HIT)
+    hits["tri"], hits["t"], hits["u"], hits["v"] = g["kd_tri"], g["kd_t"], g["kd_u"], g["kd_v"]
     acc = Accelerator("wbvh").build(tris)
-    hits = acc.intersect(rays)
     d_hits = _t(hits.view(np.int32).reshape(-1, 4))
-    n = len(rays)
     d_pos = torch.empty((n, 3), dtype=torch.float32, device="cuda")
     d_nrm = torch.empty((n, 3), dtype=torch.float32, device="cuda")
     wavefront.hit_surface(acc, d_hits, n, d_pos, d_nrm)
     torch.cuda.synchronize()
     pos, nrm = d_pos.cpu().numpy(), d_nrm.cpu().numpy()
     h = hits["tri"] >= 0
-    t = tris.reshape(-1, 3, 3)[hits["tri"][h]]
-    e1 = (t[:, 1] - t[:, 0]).astype(np.float32)
-    e2 = (t[:, 2] - t[:, 0]).astype(np.float32)
-    want_p = ((t[:, 0] + e1 * hits["u"][h][:, None]) + e2 * hits["v"][h][:, None]).astype(np.float32)
-    want_n = scenes.normalize_ref(scenes.cross_ref(e1, e2))
-    assert np.array_equal(bits(pos[h]), bits(want_p))
-    assert np.array_equal(bits(nrm[h]), bits(want_n))
+    assert h.sum() > 500
+    assert np.array_equal(bits(pos[h]), bits(s["surf_pos"][h]))
+    assert np.array_equal(bits(nrm[h]), bits(s["surf_nrm"][h]))
     assert np.all(np.isnan(pos[~h]))
+    acc.destroy()
+
+
+def test_diffuse_rays_follow_the_reference_lobe(gpu):
+    """diffuse_kernel's directions have randDirectionSuperN's distribution
+    (Common.cpp:144-182): cos^2(theta) about the facing normal uniform on
+    [0.001, 1), azimuth uniform.  A flat two-triangle floor seen from above
+    gives every hit the normal +y, so theta and the azimuth are read directly;
+    chi-square over 20 bins each (19 degrees of freedom: 99.99th percentile
+    about 49), and the mean of cos(theta) against its exact value."""
+    import torch
+    s = 1000.0
+    floor = np.array([[0, 0, 0, s, 0, 0, s, 0, s], [0, 0, 0, s, 0, s, 0, 0, s]], np.float32)
+    acc = Accelerator("wbvh").build(floor)
+    w = h = 256
+    d_prim = torch.empty((w * h, 8), dtype=torch.float32, device="cuda")
+    wavefront.camera_rays((0.5 * s, 2.0 * s, 0.5 * s), (0.5 * s, 0.0, 0.5 * s), (0.0, 0.0, 1.0), 25.0,
+                          w, h, d_prim)
+    d_hits = torch.empty((w * h, 4), dtype=torch.int32, device="cuda")
+    acc.intersect_device(d_prim, w * h, d_hits)
+    k = 4
+    d_out = torch.empty((w * h * k, 8), dtype=torch.float32, device="cuda")
+    wavefront.diffuse_rays(acc, d_prim, d_hits, w * h, k, 2024, 0.1, d_out)
+    torch.cuda.synchronize()
+    hit = np.repeat(d_hits[:, 0].cpu().numpy() >= 0, k)
+    assert hit.all()
+    d = d_out.cpu().numpy()[:, 4:7].astype(np.float64)
+    ct = d[:, 1]  # the facing normal is +y (the camera is above the floor)
+    assert ct.min() >= np.sqrt(0.001) - 1e-6
+    n = len(ct)
+    lo = 0.001
+    mean_ct = (2.0 / 3.0) * (1 - lo ** 1.5) / (1 - lo)
+    assert abs(ct.mean() - mean_ct) < 5 * np.sqrt((0.5 * (1 + lo) - mean_ct ** 2) / n)
+    edges = np.linspace(lo, 1.0, 21)
+    obs, _ = np.histogram(ct ** 2, bins=edges)
+    exp = n / 20.0
+    assert ((obs - exp) ** 2 / exp).sum() < 60.0
+    phi = np.arctan2(d[:, 2], d[:, 0])
+    obs, _ = np.histogram(phi, bins=np.linspace(-np.pi, np.pi, 21))
+    assert ((obs - exp) ** 2 / exp).sum() < 60.0
+    acc.destroy()
 
 
 def test_diffuse_rays_well_formed_and_seeded(gpu):

@@ -98,3 +98,55 @@ def test_f64_oracle_agrees_with_fp32_at_x1000():
     assert np.array_equal(f64["tri"], g["kd_tri"])
     m = f64["tri"] >= 0
     np.testing.assert_allclose(f64["t"][m], g["kd_t"][m], rtol=1e-5)
+
+
+# ---- f2: ray generation and hit surfaces ------------------------------------
+
+def _camera_cases():
+    g = np.load(GOLD / "camera_surface.npz")
+    for i in range(int(g["ncams"])):
+        p = g[f"cam{i}_params"]
+        yield (tuple(p[0:3]), tuple(p[3:6]), tuple(p[6:9]), float(p[9]), int(p[10]),
+               int(p[11])), g[f"cam{i}_rays"]
+
+
+def test_camera_restatement_matches_reference_golden():
+    """scenes.camera_rays (the host restatement of RayTracer::CalcEyeRaySamples
+    with Camera::CalcCamVectors) equals, bit for bit, the rays the reference's
+    own Camera and Vector3 code produced (tests/golden/camera_surface.npz)."""
+    for (eye, look, up, fov, w, h), want in _camera_cases():
+        got = scenes.camera_rays(w, h, eye=np.array(eye), look=np.array(look), up=up, fov_deg=fov)
+        assert np.array_equal(bits(got[:, :7]), bits(want[:, :7])), (eye, look, up)
+        assert np.all(np.isinf(got[:, 7])) and np.all(np.isinf(want[:, 7]))
+
+
+def test_camera_golden_matches_live_reference(ref_lib):
+    for (eye, look, up, fov, w, h), want in _camera_cases():
+        live = ob.ref_camera_rays(eye, look, up, fov, w, h)
+        assert np.array_equal(bits(live), bits(want))
+
+
+def test_surface_restatement_matches_reference_golden():
+    """Hit point v0 + (v1-v0)*alpha + (v2-v0)*beta and normal
+    Normalize(Cross(edge1, edge2)) restated in FP32 equal what the reference's
+    TrianglePrim::intersect stored for the Kdtree's hits."""
+    g = np.load(GOLD / "random2k_x1000.npz")
+    s = np.load(GOLD / "camera_surface.npz")
+    ids, u, v = g["kd_tri"], g["kd_u"], g["kd_v"]
+    h = ids >= 0
+    t = g["tris"].reshape(-1, 3, 3)[ids[h]]
+    e1 = (t[:, 1] - t[:, 0]).astype(np.float32)
+    e2 = (t[:, 2] - t[:, 0]).astype(np.float32)
+    p = ((t[:, 0] + e1 * u[h][:, None]) + e2 * v[h][:, None]).astype(np.float32)
+    n = scenes.normalize_ref(scenes.cross_ref(e1, e2))
+    assert np.array_equal(bits(p), bits(s["surf_pos"][h]))
+    assert np.array_equal(bits(n), bits(s["surf_nrm"][h]))
+    assert np.all(np.isnan(s["surf_pos"][~h]))
+
+
+def test_surface_golden_matches_live_reference(ref_lib):
+    g = np.load(GOLD / "random2k_x1000.npz")
+    s = np.load(GOLD / "camera_surface.npz")
+    pos, nrm = ob.ref_hit_surface(g["tris"], g["rays"], g["kd_tri"])
+    assert np.array_equal(bits(pos), bits(s["surf_pos"]))
+    assert np.array_equal(bits(nrm), bits(s["surf_nrm"]))
