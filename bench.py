@@ -11,12 +11,16 @@ Workload (one step = one pass of the closest-hit kernel over one batch):
   also   as many any-hit shadow rays toward a 0.1 x 0.1 light at height 2.0
          (reported as anyhit_mrays_s).
 
-value: Mrays/s with rays and hits resident in HBM; timed with CUDA events on
-the launch stream, L2 flushed (256 MiB write) between timed steps; max over
-ranks; whole-job aggregate.  e2e: the same through the host-buffer C-ABI call
-(enc_intersect_closest) from pinned host memory, copies inside the timed
-region.  --gpus N runs N independent replicas (one process per GPU, each with
-its own seeded batch, no collective on the data path).
+value: Mrays/s with rays and hits resident in HBM; one step = the binning
+pass (enc_bin_rays: a counting sort of the batch by origin and direction
+cell) + the closest-hit launch over the binned order
+(enc_intersect_closest_device_ordered), both inside the timed region;
+timed with CUDA events on the launch stream, L2 flushed (256 MiB write)
+between timed steps; max over ranks; whole-job aggregate.  --no-bin times
+the unbinned launch instead.  e2e: the same metric through the host-buffer
+C-ABI call (enc_intersect_closest) from pinned host memory, copies inside
+the timed region.  --gpus N runs N independent replicas (one process per
+GPU, each with its own seeded batch, no collective on the data path).
 
 --impl reference times the reference's own CPU Kdtree::intersect
 (oracle/_ref/libencore_ref.so, compiled from the reference sources; the C
@@ -44,7 +48,7 @@ RES = 1024
 LIGHT = np.array([0.5, 2.0, 0.5]) * SCALE
 METRIC = "Mrays/s incoherent closest-hit, 2M tris"
 WORKLOAD = "heightfield1024_x1000_4M_incoherent"
-CPU_SAMPLE = 65536  # rays per CPU step: 16384 primaries + 3 secondaries each
+CPU_SAMPLE = 65536  # rays per CPU step, drawn from the bench batch
 
 
 def log(*a):
@@ -186,19 +190,21 @@ def cpu_reference_rate(tris, rays_sample, steps: int = 1, warmup: int = 0):
     return rate, kind, nthreads, build_s, times
 
 
-def cpu_sample(tris, prim_res: int = 128, seed: int = 7) -> np.ndarray:
-    """CPU_SAMPLE rays of the same mix: primaries of a prim_res^2 camera over
-    the same view, their hits from the CPU reference path, 3 secondaries each."""
+def cpu_sample(tris, batch: np.ndarray | None = None, seed: int = 7) -> np.ndarray:
+    """CPU_SAMPLE rays drawn (seeded, without replacement) from the bench's
+    own 4,179,838-ray batch.  Without `batch` (the reference arm, which runs
+    no engine code) the batch is rebuilt the same way with the primaries'
+    hits from the reference's Kdtree instead of the engine's."""
     from oracle import bindings as ob
-    from encore_b200 import scenes
-    prim = scenes.camera_rays(prim_res, prim_res, eye=np.array([0.5, 1.3, 0.5]) * SCALE,
-                              look=np.array([0.5, 0.0, 0.5]) * SCALE, up=(0.0, 0.0, 1.0),
-                              fov_deg=40.0)
-    if ob.reference() is not None:
-        hits, _ = ob.ref_closest(tris, prim, kind=0)
-    else:
-        hits = ob.PortKd(tris).closest(prim, clamp=True)
-    return mixed_batch(tris, prim, hits, seed)[:CPU_SAMPLE]
+    if batch is None:
+        prim = primary_rays(RES)
+        if ob.reference() is not None:
+            hits, _ = ob.ref_closest(tris, prim, kind=0)
+        else:
+            hits = ob.PortKd(tris).closest(prim, clamp=True)
+        batch = mixed_batch(tris, prim, hits, seed=101)
+    sel = np.sort(np.random.default_rng(seed).choice(len(batch), CPU_SAMPLE, replace=False))
+    return np.ascontiguousarray(batch[sel])
 
 
 def run_reference_arm(args, rank: int, world: int) -> None:
@@ -216,9 +222,10 @@ def run_reference_arm(args, rank: int, world: int) -> None:
         "config": {"workload": WORKLOAD, "sample_rays_per_step": int(len(sample)),
                    "accelerator": "reference Kdtree (spatial median)"},
         "cpu_baseline": {"value": round(rate, 6), "unit": "Mrays/s", "cores": cores, "kind": kind,
-                         "sample": f"{len(sample)} rays of the 1:3 primary/diffuse mix per step, "
-                                   f"Kdtree::intersect on {cores} host threads; build "
-                                   f"{build_s:.1f} s not timed"},
+                         "sample": f"{len(sample)} rays per step drawn at random from the "
+                                   f"4,179,838-ray batch (primaries' hits from the reference's "
+                                   f"own Kdtree), Kdtree::intersect on {cores} host threads; "
+                                   f"build {build_s:.1f} s not timed"},
         "e2e": {"value": round(rate, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -228,14 +235,58 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 # ---------------------------------------------------------------------------
 # GPU arm
 
-def read_profile_traffic() -> float | None:
-    p = ROOT / "profiles" / "wbvh_closest_heightfield_traffic.txt"
+TRAFFIC_PROFILE = "profiles/wbvh_closest_heightfield_traffic.txt"
+
+
+def read_profile_traffic() -> dict:
+    """Per-ray DRAM and L2 figures of the closest-hit launch from the
+    committed ncu summary (keys: dram_bytes_per_ray, l2_bytes_per_ray,
+    l2_pct_of_peak, binned)."""
+    p = ROOT / TRAFFIC_PROFILE
+    out = {}
     if not p.exists():
-        return None
+        return out
     for ln in p.read_text().splitlines():
-        if ln.startswith("dram_bytes_per_ray:"):
-            return float(ln.split(":", 1)[1])
-    return None
+        if ":" in ln and not ln.startswith("#"):
+            k, v = ln.split(":", 1)
+            try:
+                out[k.strip()] = float(v)
+            except ValueError:
+                pass
+    return out
+
+
+MISMATCH_FIXTURE = "tests/golden/fullsize_mismatches.npz"
+
+
+def parity_vs_kd(got: np.ndarray, kd: np.ndarray) -> dict:
+    """Rays of the bench batch whose closest-hit triangle differs between the
+    engine and the kd-tree parity mode (the reference Kdtree's own walk,
+    bit-exact with Kdtree::intersect), checked against the committed,
+    classified list of those rays (tests/golden/make_fullsize_mismatches.py
+    made it and classified each ray with the oracle).  got, kd: (n, 4) int32
+    hit records."""
+    mism = np.nonzero(got[:, 0] != kd[:, 0])[0]
+    same = got[:, 0] == kd[:, 0]
+    out = {"vs": "reference Kdtree walk (kd-tree parity mode, bit-exact with Kdtree::intersect)",
+           "rays": int(len(got)), "mismatches": int(len(mism)),
+           "t_bits_equal_where_ids_agree": bool(np.array_equal(got[same, 1], kd[same, 1]))}
+    fx = ROOT / MISMATCH_FIXTURE
+    if not fx.exists():
+        out["mismatch_by_class"] = None
+        return out
+    g = np.load(fx)
+    idx, cls, names = g["x1000_idx"], g["x1000_cls"], g["classes"]
+    listed = (np.array_equal(mism, idx) and np.array_equal(got[mism, 0], g["x1000_got"]["tri"])
+              and np.array_equal(kd[mism, 0], g["x1000_want"]["tri"]))
+    known = np.isin(mism, idx)
+    pos = np.searchsorted(idx, mism[known])
+    counts = {}
+    for k in cls[pos]:
+        counts[str(names[k])] = counts.get(str(names[k]), 0) + 1
+    out.update({"matches_committed_list": bool(listed), "mismatch_by_class": counts,
+                "unlisted": int((~known).sum()), "list": MISMATCH_FIXTURE})
+    return out
 
 
 def c0_section(dev: int, args, flush) -> dict:
@@ -304,9 +355,9 @@ def batched_section(dev: int, args, flush) -> dict:
     tris, rays = scenes.multi_scene_workload(64, seed=33, scale=SCALE)
     total = sum(len(r) for r in rays)
     tune_idx = list(range(0, 64, 4))
-    rep = autotune([tris[i] for i in tune_idx], [rays[i] for i in tune_idx], widths=(4, 8),
-                   chunks=(16, 32, 64), blocks_per_sm=(8, 10), block_threads=(128,), reps=3,
-                   device=dev)
+    rep = autotune([tris[i] for i in tune_idx], [rays[i] for i in tune_idx], widths=(2, 4, 8),
+                   chunks=(16, 32, 64), blocks_per_sm=(8, 10), block_threads=(64, 128),
+                   stack_depths=(0, 16, 24), reps=3, device=dev, out=args.tune_table)
     width, lc = launch_config(rep["best"])
     accs8 = [Accelerator("wbvh", width=8, device=dev).build(t) for t in tris]
     accs = accs8 if width == 8 else [Accelerator("wbvh", width=width, device=dev).build(t)
@@ -353,8 +404,12 @@ def batched_section(dev: int, args, flush) -> dict:
             "rays": total, "plain_mrays_s": round(out["plain"], 1),
             "batched_mrays_s": round(out["batched"], 1),
             "batched_over_plain": round(out["batched"] / out["plain"], 3),
-            "same_hits": bool(same), "tuned": rep["best"], "launches_plain": 64,
-            "launches_batched": 1}
+            "same_hits": bool(same), "tuned": rep["best"],
+            "tuner": {"configs": rep["configs"], "stopped_at_stack_bound":
+                      rep["configs_stopped_at_stack_bound"], "all_same_hits": rep["all_same_hits"],
+                      "space": "width 2/4/8 x chunk 16/32/64 x blocks/SM 8/10 x block 64/128 x "
+                               "stack 0 (tree depth)/16/24"},
+            "launches_plain": 64, "launches_batched": 1}
 
 
 def served_section(dev: int, args) -> dict:
@@ -436,8 +491,8 @@ def served_section(dev: int, args) -> dict:
     same = all(np.array_equal(out_view(p).view(np.uint8), ref.view(np.uint8))
                for p, ref in zip(pool, plain_ref))
 
-    # latency under Poisson arrivals (ring of pooled requests, 3 passes)
-    nreq = 3 * npool
+    # latency under Poisson arrivals (the pooled requests reused as a ring)
+    nreq = max(args.served_requests, npool)
     mean_rays = total / npool
     lam = 0.6 * served_rate * 1e6 / mean_rays  # requests per second
     gaps = rng.exponential(1.0 / lam, nreq)
@@ -482,7 +537,7 @@ def served_section(dev: int, args) -> dict:
     lat = np.array(lat) * 1e3
     plain_lat = np.array(plain_lat) * 1e3
     sizes = np.array(sizes)
-    m1 = (sizes >= (512 << 10)) & (sizes <= (2 << 20))
+    m1 = (sizes >= (512 << 10)) & (sizes <= (2 << 20))  # "1M-ray requests": 0.5M-2M rays
     for a in accs:
         a.destroy()
     return {"workload": "32 resident scenes (16 random 1k-2M tris, 16 heightfields 2.1M tris), "
@@ -494,20 +549,109 @@ def served_section(dev: int, args) -> dict:
             "p50_ms": round(float(np.percentile(lat, 50)), 3),
             "p99_ms": round(float(np.percentile(lat, 99)), 3),
             "p99_ms_1M_requests": (round(float(np.percentile(lat[m1], 99)), 3) if m1.any() else None),
+            "n_1M_requests": int(m1.sum()),
+            "1M_requests": "requests of 524,288 to 2,097,152 rays",
+            "max_ms": round(float(lat.max()), 3),
             "plain_p50_ms": round(float(np.percentile(plain_lat, 50)), 3),
             "plain_p99_ms": round(float(np.percentile(plain_lat, 99)), 3),
             "copies": "host pinned buffers, copies inside every request"}
 
 
+def _gather_variant(dev: int, args, flush, pm, pos, nrm, pw, q, qn, k, r, label) -> dict:
+    """Times one radiance gather over `pm` (a built photon map) at queries
+    q/qn (device), counts the per-query work for the roofline, checks a
+    sample against the FP64 oracle and times the reference's
+    GetRadianceEstimate on the same sample."""
+    import torch
+    from oracle import bindings as ob
+    nq = q.shape[0]
+    stream = torch.cuda.current_stream()
+    d_rgb = torch.empty((nq, 3), dtype=torch.float32, device=dev)
+    for _ in range(3):
+        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    pm.check(stream.cuda_stream)
+    ms = sum(ts) / len(ts)
+    rate = nq / (ms * 1e-3) / 1e6
+    # algorithmic bytes per query from the kernel's own counts: query position
+    # and normal in (24), rgb out (12), 24 per child box tested, 16 per
+    # photon position tested, 16 per normal read, 16 per found photon's power
+    d_vis = torch.empty((nq, 4), dtype=torch.int32, device=dev)
+    d_rgb2 = torch.empty((nq, 3), dtype=torch.float32, device=dev)
+    pm.count_visits(k, r, q, qn, nq, d_rgb2, d_vis, stream=stream.cuda_stream)
+    vis = d_vis.cpu().numpy().astype(np.float64).mean(axis=0)
+    same = bool(torch.equal(d_rgb, d_rgb2))
+    bpq = 24 + 12 + 24 * vis[0] + 16 * vis[1] + 16 * vis[2] + 16 * vis[3]
+    achieved = bpq * nq / (ms * 1e-3) / 1e9
+    pk = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(pk.read_text()) if pk.exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    sel = np.linspace(0, nq - 1, 2000).astype(int)
+    qs, qns = q.cpu().numpy()[sel], qn.cpu().numpy()[sel]
+    want, cnt = ob.port_gather(pos, nrm, pw, qs, qns, k, r)
+    got = d_rgb.cpu().numpy()[sel]
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
+    cpu = None
+    if not args.no_cpu and ob.reference() is not None:
+        import ctypes as C
+        lib = ob.reference()
+        bs = C.c_double()
+        m = len(pos)
+        h = lib.encref_pmap_create(pos.ctypes.data, nrm.ctypes.data, pw.ctypes.data, m, 0,
+                                   C.byref(bs))
+        out = np.empty((len(qs), 3), np.float32)
+        nt = os.cpu_count() or 1
+        cpu_ts = []
+        for _ in range(3):
+            t1 = time.perf_counter()
+            lib.encref_pmap_radiance(h, np.ascontiguousarray(qs).ctypes.data,
+                                     np.ascontiguousarray(qns).ctypes.data, len(qs), k, r,
+                                     out.ctypes.data, nt)
+            cpu_ts.append(time.perf_counter() - t1)
+        lib.encref_pmap_destroy(h)
+        cpu = {"value": round(len(qs) / (sum(cpu_ts) / 3) / 1e6, 6), "unit": "Mqueries/s",
+               "cores": nt, "kind": "reference", "build_seconds": round(bs.value, 2),
+               "sample": f"{len(qs)} of the same queries, PhotonMap::GetRadianceEstimate, "
+                         "mean of 3 passes"}
+        ref_rel = np.abs(got - out) / np.maximum(np.abs(out), 1e-30)
+        cpu["max_rel_err_vs_reference"] = float(ref_rel.max())
+    return {"map": label, "photons": int(len(pos)),
+            "map_bytes": int(len(pos)) * 48, "queries": int(nq), "mqueries_s": round(rate, 2),
+            "ms_per_gather": round(ms, 3), "found_mean": float(cnt.mean()),
+            "max_rel_err_vs_fp64": float(rel.max()),
+            "roofline": {"bound": "hbm", "kernel": "gather_kernel", "achieved": round(achieved, 1),
+                         "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                         "bytes_per_query": round(float(bpq), 1),
+                         "per_query": {"boxes_tested": round(float(vis[0]), 2),
+                                       "photons_tested": round(float(vis[1]), 2),
+                                       "normals_read": round(float(vis[2]), 2),
+                                       "found": round(float(vis[3]), 2)},
+                         "counting_launch_same_rgb": same},
+            "cpu_baseline": cpu}
+
+
 def gather_section(dev: int, args, flush) -> dict:
-    """Photon mapping on the 10,000-random-triangle scene: 2M photons emitted
-    from a 0.1 x 0.1 light at height 2.0 (cosine lobe, power 1/N, up to 3
-    diffuse bounces, Russian roulette at albedo 0.7) traced on the GPU, one
-    photon map, then a k = 50, r = 0.02 radiance gather at 1M primary-hit
-    points (x1000 scale: r = 20)."""
+    """Photon mapping on the 10,000-random-triangle scene (x1000): photons
+    emitted from a 0.1 x 0.1 light at height 2.0 (cosine lobe, up to 3
+    diffuse bounces, Russian roulette at albedo 0.7) and traced on the GPU,
+    then a k = 50, r = 0.02 (x1000: 20) radiance gather at 1M primary-hit
+    points, on two maps:
+      l2_resident  one map of every stored photon of 2M emitted (about 0.5M
+                   photons, 25 MB: it stays in the 126 MB L2);
+      large        the reference's indirect map, filled as EmitPhotons fills
+                   it (batches of 2M emitted until 4M indirect photons are
+                   stored; 192 MB, above L2), beside its direct map."""
     import torch
     from encore_b200 import Accelerator, scenes, wavefront
-    from oracle import bindings as ob
     t0 = time.perf_counter()
     tris = scenes.random_triangles(10000, seed=0, scale=SCALE)
     acc = Accelerator("wbvh", device=dev).build(tris)
@@ -537,67 +681,47 @@ def gather_section(dev: int, args, flush) -> dict:
     ok = d_hits[:, 0] >= 0
     q = d_p[ok][: 1 << 20].contiguous()
     qn = d_n[ok][: 1 << 20].contiguous()
-    nq = q.shape[0]
-    d_rgb = torch.empty((nq, 3), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream()
     k, r = 50, 0.02 * SCALE
-    for _ in range(3):
-        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
-    ts = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        pm.get_radiance_estimate_device(k, r, q, qn, nq, d_rgb, stream=stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ts.append(e0.elapsed_time(e1))
-    rate = nq * len(ts) / (sum(ts) * 1e-3) / 1e6
-    # parity sample against the FP64 oracle on the same photons
     pos, nrm, pw = (b[:m].cpu().numpy() for b in bufs)
-    sel = np.linspace(0, nq - 1, 2000).astype(int)
-    qs, qns = q.cpu().numpy()[sel], qn.cpu().numpy()[sel]
-    want, cnt = ob.port_gather(pos, nrm, pw, qs, qns, k, r)
-    got = d_rgb.cpu().numpy()[sel]
-    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
-    cpu = None
-    if not args.no_cpu and ob.reference() is not None:
-        import ctypes as C
-        lib = ob.reference()
-        bs = C.c_double()
-        h = lib.encref_pmap_create(pos.ctypes.data, nrm.ctypes.data, pw.ctypes.data, m, 0,
-                                   C.byref(bs))
-        out = np.empty((len(qs), 3), np.float32)
-        nt = os.cpu_count() or 1
-        t1 = time.perf_counter()
-        lib.encref_pmap_radiance(h, np.ascontiguousarray(qs).ctypes.data,
-                                 np.ascontiguousarray(qns).ctypes.data, len(qs), k, r,
-                                 out.ctypes.data, nt)
-        cpu_s = time.perf_counter() - t1
-        lib.encref_pmap_destroy(h)
-        cpu = {"value": round(len(qs) / cpu_s / 1e6, 6), "unit": "Mqueries/s", "cores": nt,
-               "kind": "reference", "build_seconds": round(bs.value, 2),
-               "sample": f"{len(qs)} of the same queries, PhotonMap::GetRadianceEstimate"}
-        ref_rel = np.abs(got - out) / np.maximum(np.abs(out), 1e-30)
-        cpu["max_rel_err_vs_reference"] = float(ref_rel.max())
+    small = _gather_variant(dev, args, flush, pm, pos, nrm, pw, q, qn, k, r,
+                            "every stored photon of 2M emitted (one map)")
+    small.update({"photons_emitted": nph, "photon_trace_ms": round(trace_s * 1e3, 2),
+                  "photon_map_build_s": round(build_s, 3)})
     pm._destroy()
+    del bufs
+    torch.cuda.empty_cache()
+    # the large map: EmitPhotons' loop until the indirect map is full
+    cap_i, cap_d = 4_000_000, 16_000_000
+    ind = tuple(torch.empty((cap_i, 3), dtype=torch.float32, device=dev) for _ in range(3)) + (None,)
+    dirm = tuple(torch.empty((cap_d, 3), dtype=torch.float32, device=dev) for _ in range(3)) + (None,)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    nd, ni, emitted = wavefront.trace_photon_maps(
+        acc, LIGHT, 0.1 * SCALE, nph, dirm, ind, max_bounces=3, albedo=0.7, seed=8,
+        emit_offset=0.01 * SCALE, bounce_offset=0.001 * SCALE, shadow_offset=2.0 * SCALE,
+        fill_indirect=True)
+    fill_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    pmi = wavefront.photon_map_from_device(ind[0], ind[1], ind[2], ni, device=dev)
+    build_i = time.perf_counter() - t1
+    posi, nrmi, pwi = (b[:ni].cpu().numpy() for b in ind[:3])
+    large = _gather_variant(dev, args, flush, pmi, posi, nrmi, pwi, q, qn, k, r,
+                            "indirect map filled to 4M photons (EmitPhotons' loop)")
+    large.update({"photons_emitted": int(emitted), "direct_map_photons": int(nd),
+                  "indirect_map_photons": int(ni), "photon_trace_ms": round(fill_s * 1e3, 1),
+                  "photon_map_build_s": round(build_i, 3)})
+    pmi._destroy()
     acc.destroy()
-    log(f"gather section in {time.perf_counter() - t0:.1f}s: {m} photons stored, {nq} queries")
-    return {"workload": "10k random triangles x1000, 2M photons (<=3 bounces, RR 0.7), "
-                        "k=50 r=0.02 (x1000) at primary hits",
-            "photons_emitted": nph, "photons_stored": int(m),
-            "photon_trace_ms": round(trace_s * 1e3, 2), "photon_map_build_s": round(build_s, 3),
-            "queries": int(nq), "mqueries_s": round(rate, 2),
-            "ms_per_gather": round(sum(ts) / len(ts), 3),
-            "found_mean": float(cnt.mean()),
-            "max_rel_err_vs_fp64": float(rel.max()), "cpu_baseline": cpu}
+    log(f"gather section in {time.perf_counter() - t0:.1f}s: {m} / {ni} photons, {q.shape[0]} queries")
+    return {"workload": "10k random triangles x1000, photons traced on the GPU (<=3 bounces, "
+                        "RR 0.7), k=50 r=0.02 (x1000) at 1M primary hits",
+            "mqueries_s": small["mqueries_s"], "l2_resident": small, "large": large}
 
 
 def run_engine_arm(args, rank: int, world: int) -> None:
     import torch
     import torch.distributed as dist
-    from encore_b200 import Accelerator, HIT_DTYPE, LaunchConfig, replicas
+    from encore_b200 import Accelerator, BinConfig, HIT_DTYPE, LaunchConfig, replicas
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -627,25 +751,44 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     d_shadow = torch.from_numpy(shadow).to(dev)
     d_occ = torch.empty(n, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    binning = None if args.no_bin else BinConfig(args.bin_origin, args.bin_dir, args.bin_probe)
+    scratch = (torch.empty(acc.bin_scratch_bytes(n, binning), dtype=torch.uint8, device=dev)
+               if binning else None)
 
-    def closest():
-        acc.intersect_device(d_rays, n, d_hits, launch=launch, stream=stream)
+    def closest(mid=None):
+        """One step: bin the batch, then trace it in the binned order (mid:
+        an event recorded between the two, so the traversal launch alone is
+        timed too)."""
+        if binning is None:
+            if mid is not None:
+                mid.record(stream)
+            acc.intersect_device(d_rays, n, d_hits, launch=launch, stream=stream)
+            return
+        order = acc.bin_rays(d_rays, n, scratch, binning, stream=stream)
+        if mid is not None:
+            mid.record(stream)
+        acc.intersect_device_ordered(d_rays, n, order, d_hits, launch=launch, stream=stream)
 
-    def anyhit():
+    def anyhit(mid=None):
+        if mid is not None:
+            mid.record(stream)
         acc.occluded_device(d_shadow, n, d_occ, launch=launch, stream=stream)
 
     def timed(fn, steps):
+        """Per step (whole step ms, traversal launch ms), CUDA events on the
+        launch stream, L2 flushed before each step."""
         evs = []
         for _ in range(steps):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
+            m = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            fn()
+            fn(m)
             b.record(stream)
-            evs.append((a, b))
+            evs.append((a, m, b))
         torch.cuda.synchronize()
-        return [a.elapsed_time(b) for a, b in evs]
+        return ([a.elapsed_time(b) for a, m, b in evs], [m.elapsed_time(b) for a, m, b in evs])
 
     for _ in range(args.warmup):
         closest()
@@ -656,19 +799,21 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    ms = timed(closest, args.steps)
+    ms, ms_trace = timed(closest, args.steps)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
     acc.check(stream)
-    ms_any = timed(anyhit, args.steps)
+    ms_any, _ = timed(anyhit, args.steps)
     acc.check(stream)
 
     # whole-job rate: every replica's rays over the slowest replica's device time
     rate, total_ms = replicas.aggregate_rate(n, args.steps, sum(ms))
     any_rate, _ = replicas.aggregate_rate(n, args.steps, sum(ms_any))
+    _, trace_total_ms = replicas.aggregate_rate(n, args.steps, sum(ms_trace))
     ms_step = total_ms / args.steps
+    ms_trace_step = trace_total_ms / args.steps
     value = rate / 1e6
     any_value = any_rate / 1e6
 
@@ -677,23 +822,30 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     assert np.array_equal(got[:, 0], hits_ref["tri"]), "timed kernel output differs"
 
     # the kd-tree parity mode (the reference Kdtree's own cells and order,
-    # bit-exact with it) on the same batch, for scale against the wide BVH
+    # bit-exact with it) on the same batch, for scale against the wide BVH,
+    # and the list of rays whose triangle differs between the two
     kd_value = None
+    parity = None
     if not args.no_extras:
         t_kd = time.perf_counter()
         kd = Accelerator("kdtree", device=dev).build(tris)
         kd_build_s = time.perf_counter() - t_kd
 
-        def kd_closest():
+        def kd_closest(mid=None):
+            if mid is not None:
+                mid.record(stream)
             kd.intersect_device(d_rays, n, d_hits, launch=None, stream=stream)
 
         for _ in range(2):
             kd_closest()
-        ms_kd = timed(kd_closest, max(1, args.steps // 4))
+        ms_kd, _ = timed(kd_closest, max(1, args.steps // 4))
         kd.check(stream)
         kd_rate, _ = replicas.aggregate_rate(n, len(ms_kd), sum(ms_kd))
         kd_value = {"mrays_s": round(kd_rate / 1e6, 3), "build_seconds": round(kd_build_s, 2)}
+        kd_hits = d_hits.cpu().numpy().view(np.int32)
         kd.destroy()
+        if rank == 0:
+            parity = parity_vs_kd(got, kd_hits)
 
     # algorithmic bytes per ray from the engine's own traversal counts
     d_vis = torch.empty((n, 2), dtype=torch.int32, device=dev)
@@ -703,7 +855,7 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     nodes_per_ray = vis[:, 0].mean()
     tris_per_ray = vis[:, 1].mean()
     bytes_per_ray = 32 + 16 + nodes_per_ray * node_b + tris_per_ray * 48
-    launch_s = ms_step * 1e-3
+    launch_s = ms_trace_step * 1e-3  # the traversal launch alone
     achieved = bytes_per_ray * n / launch_s / 1e9
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
@@ -711,7 +863,11 @@ def run_engine_arm(args, rank: int, world: int) -> None:
         peaks = json.loads(pk.read_text())
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    dram_per_ray = read_profile_traffic()
+    prof = read_profile_traffic()
+    dram_per_ray = prof.get("dram_bytes_per_ray")
+    bin_ms = ms_step - ms_trace_step
+    # binning: ray read (32) + key write (4) + key read (4) + order write (4)
+    bin_bytes = 44 * n
 
     # e2e: host-buffer C-ABI call, pinned buffers, copies inside the timed region
     h_rays = torch.from_numpy(rays).pin_memory()
@@ -735,13 +891,12 @@ def run_engine_arm(args, rank: int, world: int) -> None:
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        sample = cpu_sample(tris)
-        rate, kind, cores, build_s, _ = cpu_reference_rate(tris, sample, steps=1, warmup=0)
+        sample = cpu_sample(tris, rays)
+        rate, kind, cores, build_s, _ = cpu_reference_rate(tris, sample, steps=3, warmup=1)
         cpu = {"value": round(rate, 6), "unit": "Mrays/s", "cores": cores, "kind": kind,
-               "sample": f"{len(sample)} rays of the same 1:3 primary/diffuse mix (16384 "
-                         f"primaries of a 128x128 camera + 3 secondaries each), reference "
-                         f"Kdtree::intersect on {cores} host threads; Kdtree build "
-                         f"{build_s:.1f} s not timed"}
+               "sample": f"{len(sample)} rays drawn at random from the timed {n}-ray batch, "
+                         f"reference Kdtree::intersect on {cores} host threads, mean of 3 passes "
+                         f"after 1 untimed; Kdtree build {build_s:.1f} s not timed"}
 
     acc.destroy()
     del d_rays, d_hits, d_shadow, d_occ, h_rays, h_hits
@@ -767,14 +922,30 @@ def run_engine_arm(args, rank: int, world: int) -> None:
                        f"wbvh{info['width']} quantised 8-bit, leaf<={args.leaf}",
                        "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": args.steps,
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+            "gpu_launches": args.steps * (1 if binning is None else 4),
+            "roofline": {"bound": "hbm", "kernel": "wbvh_trace (closest hit)",
+                         "achieved": round(achieved, 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(achieved / hbm, 4),
                          "peak_source": peak_src,
+                         "launch_ms": round(ms_trace_step, 4),
                          "traffic": (round(dram_per_ray * n) if dram_per_ray else None),
+                         "traffic_source": (f"{TRAFFIC_PROFILE} (ncu capture, per ray x rays)"
+                                            if dram_per_ray else None),
+                         "l2": ({"bytes": round(prof["l2_bytes_per_ray"] * n),
+                                 "achieved_gbs": round(prof["l2_bytes_per_ray"] * n / launch_s / 1e9, 1),
+                                 "pct_of_peak": prof.get("l2_pct_of_peak"),
+                                 "source": f"{TRAFFIC_PROFILE} (ncu capture)"}
+                                if "l2_bytes_per_ray" in prof else None),
                          "bytes_per_ray": round(bytes_per_ray, 1),
                          "nodes_per_ray": round(float(nodes_per_ray), 2),
                          "tris_per_ray": round(float(tris_per_ray), 2)},
+            "binning": ({"ms": round(bin_ms, 4), "bytes_per_ray": 44,
+                         "achieved_gbs": round(bin_bytes / (bin_ms * 1e-3) / 1e9, 1)
+                         if bin_ms > 0 else None,
+                         "key_bits": {"origin": args.bin_origin, "dir": args.bin_dir},
+                         "probe_frac": args.bin_probe}
+                        if binning is not None else None),
+            "parity": parity,
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(rays.nbytes), "d2h_bytes_per_step": int(n * 16)},
             "anyhit_mrays_s": round(any_value, 3),
@@ -802,6 +973,14 @@ def main():
     ap.add_argument("--bps", type=int, default=0)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--stack", type=int, default=0)
+    ap.add_argument("--no-bin", action="store_true",
+                    help="time the unbinned closest-hit launch (no binning pass)")
+    ap.add_argument("--bin-origin", type=int, default=0, help="binning key: origin bits (0 = default)")
+    ap.add_argument("--bin-dir", type=int, default=0, help="binning key: direction bits")
+    ap.add_argument("--bin-probe", type=float, default=0.0,
+                    help="binning key: probe distance as a fraction of the scene diagonal")
+    ap.add_argument("--tune-table", default=None,
+                    help="batched section: write the autotuner's sweep table (JSON) here")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched multi-scene, served and photon-gather sections")
@@ -809,6 +988,8 @@ def main():
                     help="served section: request slots (rounds in flight)")
     ap.add_argument("--server-slot-rays", type=int, default=4 << 20,
                     help="served section: ray capacity of a slot (>= the largest request, 4M)")
+    ap.add_argument("--served-requests", type=int, default=1200,
+                    help="served section: Poisson arrivals behind the latency percentiles")
     ap.add_argument("--served-only", action="store_true",
                     help="run only the served section (prints its JSON object)")
     ap.add_argument("--gather-only", action="store_true",

@@ -143,6 +143,10 @@ SIGNATURES = {
     "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_bin_scratch_bytes": (C.c_int32, [C.c_size_t, C.POINTER(BinOpts),
                                           C.POINTER(C.c_size_t)]),
+    "enc_bin_rays": (C.c_int32, [P, P, C.c_size_t, P, C.c_size_t, C.POINTER(BinOpts),
+                                 C.POINTER(C.c_void_p), P]),
+    "enc_intersect_closest_device_ordered": (C.c_int32, [P, P, C.c_size_t, P, P,
+                                                         C.POINTER(LaunchOpts), P]),
     "enc_intersect_closest_device_binned": (C.c_int32, [P, P, C.c_size_t, P, P, C.c_size_t,
                                                         C.POINTER(BinOpts),
                                                         C.POINTER(LaunchOpts), P]),
@@ -174,6 +178,9 @@ SIGNATURES = {
     "enc_photons_trace_maps_device": (C.c_int32, [P, C.POINTER(PhotonOpts), C.c_float, C.c_int32,
                                                   C.POINTER(PhotonStore), C.POINTER(PhotonStore),
                                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P]),
+    "enc_photons_trace_maps": (C.c_int32, [P, C.POINTER(PhotonOpts), C.c_float, C.c_int32,
+                                           C.POINTER(PhotonStore), C.POINTER(PhotonStore),
+                                           C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P]),
     "enc_photonmap_create_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32,
                                                 C.POINTER(P)]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),

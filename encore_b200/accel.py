@@ -173,6 +173,26 @@ class Accelerator:
             self.handle, ptr(d_rays), n, ptr(d_hits), ptr(d_scratch), nbytes, C.byref(b),
             C.byref(lo), _stream_ptr(stream)), "enc_intersect_closest_device_binned")
 
+    def bin_rays(self, d_rays, n: int, d_scratch, binning: BinConfig | None = None,
+                 stream=None) -> int:
+        """Enqueues the binning pass alone; returns the device address of the
+        permutation (inside d_scratch) for intersect_device_ordered."""
+        b = (binning or BinConfig()).c()
+        nbytes = d_scratch.numel() * d_scratch.element_size()
+        order = C.c_void_p()
+        check(self.lib.enc_bin_rays(self.handle, ptr(d_rays), n, ptr(d_scratch), nbytes,
+                                    C.byref(b), C.byref(order), _stream_ptr(stream)),
+              "enc_bin_rays")
+        return order.value or 0
+
+    def intersect_device_ordered(self, d_rays, n: int, d_order, d_hits,
+                                 launch: LaunchConfig | None = None, stream=None) -> None:
+        """Closest hit taking ray d_order[q] as the q-th ray of the queue."""
+        lo = (launch or LaunchConfig()).c()
+        check(self.lib.enc_intersect_closest_device_ordered(
+            self.handle, ptr(d_rays), n, ptr(d_order), ptr(d_hits), C.byref(lo),
+            _stream_ptr(stream)), "enc_intersect_closest_device_ordered")
+
     def occluded_device(self, d_rays, n: int, d_occ, launch: LaunchConfig | None = None,
                         stream=None) -> None:
         lo = (launch or LaunchConfig()).c()

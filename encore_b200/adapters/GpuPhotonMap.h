@@ -142,4 +142,50 @@ class GpuPhotonMap {
   enc_status m_status;
 };
 
+// PhotonMapperCPU::EmitPhotons (PhotonMapperCPU.cpp:503-586) on the device
+// for a scene of diffuse surfaces: photons from the square light in `opts`
+// traced by enc_photons_trace_maps, and stored where ReflectPhotonDiffusely
+// and EmitShadowPhoton store them (PhotonMapperCPU.cpp:701-745, 776-798):
+// first hits and shadow photons (shadowOffset > 0; the reference's offset
+// is 2 at unit scale) into `direct`, later bounces into `indirect`.  With
+// fillIndirect, batches of opts.nphotons are emitted until `indirect` is
+// full, as EmitPhotons loops.  Each map takes at most its free capacity; the
+// photons' power is 1 / photons emitted (the reference then rescales with
+// ScalePhotons); their direction is the light's -y.  *emitted (may be NULL)
+// receives the paths emitted.
+inline enc_status GpuEmitPhotons(enc_accel accel, const enc_photon_opts& opts,
+                                 float shadowOffset, bool fillIndirect, GpuPhotonMap& direct,
+                                 GpuPhotonMap& indirect, uint32_t* emitted) {
+  GpuPhotonMap* maps[2] = {&direct, &indirect};
+  std::vector<float> buf[2];
+  std::vector<uint32_t> tag[2];
+  enc_photon_store st[2];
+  for (int m = 0; m < 2; ++m) {
+    const size_t cap = maps[m]->GetMaxPhotons() - (size_t)maps[m]->GetCountStored();
+    buf[m].resize(9 * cap + 1);
+    tag[m].resize(cap + 1);
+    st[m].d_pos = &buf[m][0];
+    st[m].d_nrm = &buf[m][0] + 3 * cap;
+    st[m].d_pow = &buf[m][0] + 6 * cap;
+    st[m].d_tag = &tag[m][0];
+    st[m].capacity = (uint32_t)cap;
+  }
+  uint32_t stored[2] = {0, 0};
+  const enc_status s = enc_photons_trace_maps(accel, &opts, shadowOffset, fillIndirect ? 1 : 0,
+                                              &st[0], &st[1], stored, emitted, NULL);
+  if (s != ENC_OK) return s;
+  for (int m = 0; m < 2; ++m) {
+    for (uint32_t i = 0; i < stored[m]; ++i) {
+      const float* p = st[m].d_pos + 3 * i;
+      const float* n = st[m].d_nrm + 3 * i;
+      const float* w = st[m].d_pow + 3 * i;
+      Photon ph(Point3(p[0], p[1], p[2]), encore::Color(w[0], w[1], w[2]), Vector3(0.f, -1.f, 0.f));
+      ph.SurfNormal(Vector3(n[0], n[1], n[2]));
+      ph.SetShadowPhoton((tag[m][i] & 8u) != 0);
+      maps[m]->AddPhoton(ph);
+    }
+  }
+  return ENC_OK;
+}
+
 #endif  // ENCORE_B200_GPU_PHOTON_MAP_H

@@ -14,6 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
+from ._lib import EncoreError
 from .accel import Accelerator, LaunchConfig
 from .batch import BatchLaunch
 
@@ -35,7 +36,16 @@ def autotune(scene_tris: Sequence[np.ndarray], ray_batches: Sequence[np.ndarray]
             lc = LaunchConfig(block_threads=bt, blocks_per_sm=bps, chunk=ch, stack_depth=sd)
             b = BatchLaunch(list(zip(accs, d_rays, d_hits)), launch=lc)
             b.launch_graph()
-            b.check()
+            try:
+                b.check()
+            except EncoreError as e:
+                # a stack shallower than the deepest tree stops rays at its
+                # bound: the configuration is reported and never chosen
+                b.destroy()
+                results.append({"width": w, "chunk": ch, "blocks_per_sm": bps,
+                                "block_threads": bt, "stack_depth": sd, "ms": None,
+                                "mrays_s": None, "same_hits": False, "error": str(e)})
+                continue
             tri = torch.cat([h[:, 0] for h in d_hits]).cpu().numpy()
             if reference_tri is None:
                 reference_tri = tri
@@ -59,8 +69,11 @@ def autotune(scene_tris: Sequence[np.ndarray], ray_batches: Sequence[np.ndarray]
             a.destroy()
     ok = [r for r in results if r["same_hits"]]
     best = max(ok, key=lambda r: r["mrays_s"]) if ok else None
+    failed = [r for r in results if "error" in r]
     report = {"best": best, "rays": total, "scenes": len(scene_tris),
-              "all_same_hits": len(ok) == len(results), "results": results,
+              "all_same_hits": all(r["same_hits"] for r in results if "error" not in r),
+              "configs": len(results), "configs_stopped_at_stack_bound": len(failed),
+              "results": results,
               "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
     if out:
         Path(out).write_text(json.dumps(report, indent=1))

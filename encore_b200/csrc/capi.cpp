@@ -502,6 +502,63 @@ enc_status enc_bin_scratch_bytes(size_t nrays, const enc_bin_opts* bin, size_t* 
   return ENC_OK;
 }
 
+enc_status enc_bin_rays(enc_accel a, const float* d_rays, size_t nrays, void* d_scratch,
+                        size_t scratch_bytes, const enc_bin_opts* bin, uint32_t** d_order,
+                        enc_stream stream) {
+  if (!a || !d_order || (nrays && (!d_rays || !d_scratch))) {
+    set_error("enc_bin_rays: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *d_order = nullptr;
+  if (nrays > 0xffffffffull / 2) {
+    set_error("enc_bin_rays: too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int ob, db;
+  float pf;
+  if (!resolve_bin(bin, &ob, &db, &pf)) {
+    set_error("enc_bin_rays: origin_bits + dir_bits must be 1..20");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays == 0) return ENC_OK;
+  if (scratch_bytes < bin_scratch_bytes(nrays, ob + db) ||
+      (reinterpret_cast<uintptr_t>(d_scratch) & 255u) != 0) {
+    set_error("enc_bin_rays: scratch smaller than enc_bin_scratch_bytes or not 256-byte aligned");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(a->dev.device);
+  const BinSpec spec = make_bin_spec(a->dev.lo, a->dev.hi, ob + db, db, pf);
+  int e = launch_bin(d_rays, nrays, spec, d_scratch, d_order, a->dev.device, stream);
+  if (e != 0) return cuda_fail((cudaError_t)e, "binning launch");
+  return ENC_OK;
+}
+
+enc_status enc_intersect_closest_device_ordered(enc_accel a, const float* d_rays, size_t nrays,
+                                                const uint32_t* d_order, enc_hit* d_hits,
+                                                const enc_launch_opts* launch, enc_stream stream) {
+  if (!a || (nrays && (!d_rays || !d_hits || !d_order))) {
+    set_error("enc_intersect_closest_device_ordered: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (nrays > 0xffffffffull / 2) {
+    set_error("enc_intersect_closest_device_ordered: too many rays in one call");
+    return ENC_ERR_INVALID_ARG;
+  }
+  if (a->dev.kind != ENC_ACCEL_WBVH) {
+    set_error("enc_intersect_closest_device_ordered: wide BVH only");
+    return ENC_ERR_UNSUPPORTED;
+  }
+  DeviceScope ds(a->dev.device);
+  Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
+  if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 || L.chunk < 1) {
+    set_error("enc_intersect: launch options out of range (block multiple of 32 <= 128, stack 0 or 2..64)");
+    return ENC_ERR_INVALID_ARG;
+  }
+  int e = launch_closest(a->dev, d_rays, nrays, d_hits, L, stream, nullptr, d_order);
+  if (e != 0) return cuda_fail((cudaError_t)e, "closest-hit launch");
+  return ENC_OK;
+}
+
 enc_status enc_intersect_closest_device_binned(enc_accel a, const float* d_rays, size_t nrays,
                                                enc_hit* d_hits, void* d_scratch,
                                                size_t scratch_bytes, const enc_bin_opts* bin,

@@ -283,10 +283,18 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
       const unsigned rank = __popc(need & lt);
       const unsigned qoff = pool_next - pool_base + rank;  // offset of this lane's ray in the chunk
       const unsigned via = kOrdered ? __shfl_sync(kFull, ord_reg, qoff & 31u) : 0u;
+      bool bad_order = false;
       if (((need >> lane) & 1u) && rank < avail) {
         ray = (int)(pool_next + rank);
-        if (kOrdered && P.order != nullptr)
-          ray = (int)(qoff < 32u ? via : __ldg(P.order + pool_next + rank));
+        if (kOrdered && P.order != nullptr) {
+          const unsigned oi = qoff < 32u ? via : __ldg(P.order + pool_next + rank);
+          // an order entry outside the batch is skipped and reported
+          bad_order = oi >= P.nrays;
+          ray = bad_order ? -1 : (int)oi;
+        }
+      }
+      if (bad_order) atomicOr(l_status, kStatusBounds);
+      if (ray >= 0 && ((need >> lane) & 1u) && rank < avail) {
         const float4* rp;
         if constexpr (MULTI) {
           const BatchDesc& bd = P.batches[pool_batch];

@@ -652,4 +652,59 @@ enc_status enc_photons_trace_maps_device(enc_accel accel, const enc_photon_opts*
                        static_cast<cudaStream_t>(stream), "enc_photons_trace_maps_device");
 }
 
+enc_status enc_photons_trace_maps(enc_accel accel, const enc_photon_opts* o, float shadow_offset,
+                                  int32_t fill_indirect, const enc_photon_store* direct,
+                                  const enc_photon_store* indirect, uint32_t stored[2],
+                                  uint32_t* emitted, enc_stream stream) {
+  const DevAccel* a = accel_device_view(accel);
+  if (!a || !o || !stored || !direct || !indirect) return ENC_ERR_INVALID_ARG;
+  const enc_photon_store* hs[2] = {direct, indirect};
+  for (const enc_photon_store* m : hs) {
+    if (m->capacity && (!m->d_pos || !m->d_nrm || !m->d_pow)) {
+      set_error("enc_photons_trace_maps: a store with capacity needs its arrays");
+      return ENC_ERR_INVALID_ARG;
+    }
+  }
+  // device stores for the call, copied back and freed at its end
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != a->device) cudaSetDevice(a->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PhotonStore ds[2];
+  void* blocks[2] = {nullptr, nullptr};
+  cudaError_t e = cudaSuccess;
+  for (int m = 0; m < 2 && e == cudaSuccess; ++m) {
+    const size_t cap = hs[m]->capacity;
+    const size_t bytes = cap * (36 + (hs[m]->d_tag ? 4 : 0)) + 16;
+    e = cudaMalloc(&blocks[m], bytes);
+    float* base = static_cast<float*>(blocks[m]);
+    ds[m] = PhotonStore{base, base + 3 * cap, base + 6 * cap,
+                        hs[m]->d_tag ? reinterpret_cast<uint32_t*>(base + 9 * cap) : nullptr,
+                        hs[m]->capacity};
+  }
+  enc_status st = ENC_OK;
+  if (e == cudaSuccess) {
+    st = trace_photons(accel, o, 1, shadow_offset, fill_indirect ? 1 : 0, ds[0], ds[1], stored,
+                       emitted, s, "enc_photons_trace_maps");
+    for (int m = 0; m < 2 && st == ENC_OK && e == cudaSuccess; ++m) {
+      const size_t n = stored[m];
+      if (!n) continue;
+      e = cudaMemcpyAsync(hs[m]->d_pos, ds[m].pos, n * 12, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hs[m]->d_nrm, ds[m].nrm, n * 12, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hs[m]->d_pow, ds[m].pw, n * 12, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && ds[m].tag)
+        e = cudaMemcpyAsync(hs[m]->d_tag, ds[m].tag, n * 4, cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  cudaFree(blocks[0]);
+  cudaFree(blocks[1]);
+  if (prev >= 0 && prev != a->device) cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_error(std::string("enc_photons_trace_maps: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? ENC_ERR_OUT_OF_MEMORY : ENC_ERR_CUDA;
+  }
+  return st;
+}
+
 }  // extern "C"

@@ -153,3 +153,102 @@ def intersect_sharded(acc, rays: np.ndarray, dst: int | None = 0, **kw) -> np.nd
     lo, hi = ray_range(len(rays), rank, ws)
     local = acc.intersect(rays[lo:hi], **kw)
     return gather_records(local, dst=dst)
+
+
+class SceneRouter:
+    """Multi-GPU serving by scene affinity.  Every scene is resident on one
+    GPU (route_scenes, greedy by cost), each rank runs its own server
+    (encore_b200.serving.Server on its GPU) over the scenes it owns, and a
+    batch of requests submitted on the front-end rank is routed whole to the
+    scenes' owners, served there with continuous batching, and the results
+    are returned to the front end in submission order.  No ray of a request
+    is split across GPUs and no kernel reads another GPU's memory: rays go
+    to the owner and hits come back by point-to-point copies over the process
+    group (NCCL between GPUs, gloo on CPU).
+
+    server       this rank's server: add_scene(acc) -> id, submit(id, rays,
+                 kind) -> request id, wait(request id) -> (out, info)
+    build_scene  scene index -> the accelerator to make resident here (called
+                 only for the scenes this rank owns)
+    """
+
+    CLOSEST, ANY = 0, 1
+
+    def __init__(self, scene_costs, server, build_scene, front: int = 0):
+        self.rank, self.world_size = world()
+        self.owner = route_scenes(scene_costs, self.world_size)
+        self.server = server
+        self.front = front
+        self.local = {s: server.add_scene(build_scene(s))
+                      for s, o in enumerate(self.owner) if o == self.rank}
+
+    @staticmethod
+    def _out_bytes(kind: int, n: int) -> int:
+        return n * (16 if kind == SceneRouter.CLOSEST else 1)
+
+    def run(self, requests=None):
+        """Collective: every rank calls it.  `requests` (front end only): a list
+        of (scene, kind, rays), rays (n, 8) float32.  Returns, on the front
+        end, the outputs in request order (enc_hit records as (n,) HIT
+        arrays for closest hit, (n,) uint8 for any hit); None elsewhere."""
+        from .accel import HIT_DTYPE
+        rank, ws, front = self.rank, self.world_size, self.front
+        if rank == front:
+            meta = [(i, int(s), int(k), int(len(r))) for i, (s, k, r) in enumerate(requests)]
+        else:
+            meta = None
+        if _active():
+            box = [meta]
+            dist.broadcast_object_list(box, src=front)
+            meta = box[0]
+        share = {r: [m for m in meta if self.owner[m[1]] == r] for r in range(ws)}
+        dev = _device() if _active() else None
+        # rays to their owners
+        mine = share[rank]
+        nmine = sum(m[3] for m in mine)
+        if rank == front:
+            for r in range(ws):
+                if r == front or not share[r]:
+                    continue
+                buf = np.concatenate([np.ascontiguousarray(requests[m[0]][2], np.float32)
+                                      for m in share[r]]).reshape(-1)
+                dist.send(torch.from_numpy(buf).to(dev), dst=r)
+            rays_of = {m[0]: np.ascontiguousarray(requests[m[0]][2], np.float32) for m in mine}
+        else:
+            rays_of = {}
+            if mine:
+                t = torch.empty(nmine * 8, dtype=torch.float32, device=dev)
+                dist.recv(t, src=front)
+                flat = t.cpu().numpy().reshape(-1, 8)
+                off = 0
+                for m in mine:
+                    rays_of[m[0]] = flat[off:off + m[3]]
+                    off += m[3]
+        # serve this rank's share: all submitted, then all waited, so the
+        # server batches them continuously
+        rids = [(m, self.server.submit(self.local[m[1]], rays_of[m[0]], m[2])) for m in mine]
+        outs = {m[0]: self.server.wait(rid)[0] for m, rid in rids}
+        # results back to the front end, in each owner's share order
+        if rank != front:
+            if mine:
+                buf = np.concatenate([np.ascontiguousarray(outs[m[0]]).reshape(-1).view(np.uint8)
+                                      for m in mine])
+                dist.send(torch.from_numpy(buf).to(dev), dst=front)
+            return None
+        results = [None] * len(meta)
+        for m in mine:
+            results[m[0]] = outs[m[0]]
+        for r in range(ws):
+            if r == front or not share[r]:
+                continue
+            nb = sum(self._out_bytes(m[2], m[3]) for m in share[r])
+            t = torch.empty(nb, dtype=torch.uint8, device=dev)
+            dist.recv(t, src=r)
+            raw = t.cpu().numpy()
+            off = 0
+            for m in share[r]:
+                b = self._out_bytes(m[2], m[3])
+                chunk = raw[off:off + b].copy()
+                results[m[0]] = chunk.view(HIT_DTYPE) if m[2] == self.CLOSEST else chunk
+                off += b
+        return results

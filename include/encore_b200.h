@@ -230,6 +230,21 @@ typedef struct enc_bin_opts {
   float probe_frac;
 } enc_bin_opts;
 enc_status enc_bin_scratch_bytes(size_t nrays, const enc_bin_opts* bin, size_t* bytes);
+/* The two halves of the binned call, for callers that time them apart or
+ * trace one binned batch more than once.  enc_bin_rays enqueues the binning
+ * on `stream` and sets *d_order to the permutation inside d_scratch (valid
+ * until the scratch is reused).  enc_intersect_closest_device_ordered traces
+ * ray d_order[q] as the q-th ray of the queue and writes each hit at its
+ * ray's index; d_order should be a permutation of 0..nrays-1 (an entry
+ * >= nrays is skipped and reported by enc_accel_check as an index out of
+ * range). */
+enc_status enc_bin_rays(enc_accel accel, const float* d_rays, size_t nrays, void* d_scratch,
+                        size_t scratch_bytes, const enc_bin_opts* bin, uint32_t** d_order,
+                        enc_stream stream);
+enc_status enc_intersect_closest_device_ordered(enc_accel accel, const float* d_rays,
+                                                size_t nrays, const uint32_t* d_order,
+                                                enc_hit* d_hits, const enc_launch_opts* launch,
+                                                enc_stream stream);
 enc_status enc_intersect_closest_device_binned(enc_accel accel, const float* d_rays,
                                                size_t nrays, enc_hit* d_hits, void* d_scratch,
                                                size_t scratch_bytes, const enc_bin_opts* bin,
@@ -434,6 +449,14 @@ enc_status enc_photons_trace_maps_device(enc_accel accel, const enc_photon_opts*
                                          const enc_photon_store* direct,
                                          const enc_photon_store* indirect, uint32_t stored[2],
                                          uint32_t* emitted, enc_stream stream);
+/* The same with host stores (the pointers of enc_photon_store in host
+ * memory): device stores are allocated for the call, copied back and freed.
+ * GpuPhotonMap's GpuEmitPhotons fills a direct and an indirect map with it. */
+enc_status enc_photons_trace_maps(enc_accel accel, const enc_photon_opts* opts,
+                                  float shadow_offset, int32_t fill_indirect,
+                                  const enc_photon_store* direct,
+                                  const enc_photon_store* indirect, uint32_t stored[2],
+                                  uint32_t* emitted, enc_stream stream);
 /* PhotonMap over photon arrays in device memory (3 floats each per photon). */
 enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, const float* d_pow,
                                        size_t nphotons, int32_t caustic, int32_t device,

@@ -8,6 +8,7 @@ tests/, __graft_entry__.smoke() and the CPU arm of bench.py.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -16,6 +17,10 @@ import numpy as np
 ORACLE = Path(__file__).resolve().parent
 PORT_SO = ORACLE / "_ref" / "libencore_oracle.so"
 REF_SO = ORACLE / "_ref" / "libencore_ref.so"
+# The reference's source tree (read only, to compile oracle/_ref and to read
+# its shipped meshes and scene files): $ENCORE_REFERENCE_DIR, else the
+# location oracle/Makefile defaults to.
+REFERENCE_DIR = Path(os.environ.get("ENCORE_REFERENCE_DIR", "/root/reference/ENCORE"))
 
 HIT = np.dtype([("tri", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
 P = C.c_void_p

@@ -274,6 +274,37 @@ int main() {
   std::printf("photons queries %d set_diff %ld heap_bad %ld radiance_max_rel_err %.3g\n", 2 * nq,
               set_diff, heap_bad, worst);
   ok &= set_diff == 0 && heap_bad == 0 && worst <= 1e-4;
+
+  // EmitPhotons on the device into two GpuPhotonMaps (PhotonMapperCPU's
+  // direct and indirect maps): the indirect map is filled by the emission
+  // loop, the direct map holds first hits and shadow photons, and both agree
+  // with the C ABI's own split call on the same options.
+  enc_photon_opts po;
+  po.light_center[0] = 0.5f * scale;
+  po.light_center[1] = 2.0f * scale;
+  po.light_center[2] = 0.5f * scale;
+  po.light_size = 0.1f * scale;
+  po.nphotons = 20000;
+  po.max_bounces = 3;
+  po.albedo = 0.7f;
+  po.seed = 5;
+  po.emit_offset = 0.01f * scale;
+  po.bounce_offset = 0.001f * scale;
+  GpuPhotonMap direct(200000), indirect(2000);
+  uint32_t emitted = 0;
+  const enc_status es = GpuEmitPhotons(gbvh.handle(), po, 5.0f, true, direct, indirect, &emitted);
+  std::vector<float> bd(9 * 200000 + 9), bi(9 * 2000 + 9);
+  enc_photon_store sd = {&bd[0], &bd[0] + 3 * 200000, &bd[0] + 6 * 200000, NULL, 200000};
+  enc_photon_store si = {&bi[0], &bi[0] + 3 * 2000, &bi[0] + 6 * 2000, NULL, 2000};
+  uint32_t stored[2] = {0, 0}, emitted2 = 0;
+  const enc_status es2 = enc_photons_trace_maps(gbvh.handle(), &po, 5.0f, 1, &sd, &si, stored,
+                                                &emitted2, NULL);
+  std::printf("emit status %d direct %d indirect %d emitted %u abi %u %u %u\n", (int)es,
+              direct.GetCountStored(), indirect.GetCountStored(), emitted, stored[0], stored[1],
+              emitted2);
+  ok &= es == ENC_OK && es2 == ENC_OK && indirect.Full() && emitted > po.nphotons &&
+        emitted == emitted2 && (uint32_t)direct.GetCountStored() == stored[0] &&
+        (uint32_t)indirect.GetCountStored() == stored[1] && stored[0] > 0;
   std::printf("result %s\n", ok ? "pass" : "fail");
   return ok ? 0 : 1;
 }

@@ -96,10 +96,6 @@ def test_budget_capacity_and_cancel(gpu):
     tiny.destroy()
     srv = Server(slots=1, slot_rays=1 << 16)
     sid = srv.add_scene(accs[2])
-    big = np.zeros(((1 << 16) + 1, 8), np.float32)
-    with pytest.raises(EncoreError) as ei:
-        srv.submit(sid, big)
-    assert ei.value.status == 5
     reqs = _requests(tris[2:3], 12, seed=901, max_rays=60000)
     rids = [srv.submit(sid, r, k) for _, k, r in reqs]
     cancelled = [rid for rid in rids[-4:] if srv.cancel(rid)]
@@ -121,3 +117,63 @@ def test_empty_request_and_timeout(gpu):
     out, info = srv.wait(srv.submit(sid, np.zeros((0, 8), np.float32)))
     assert len(out) == 0 and info["nrays"] == 0
     srv.destroy()
+
+
+def test_request_larger_than_a_slot_is_split_and_identical(gpu):
+    """A request of more rays than one slot holds runs as slot-sized pieces
+    over several rounds, mixed with other requests; its hits equal the plain
+    call's, and so do the small requests' around it."""
+    tris, accs = _pool()
+    srv = Server(slots=2, slot_rays=1 << 14)
+    ids = [srv.add_scene(a) for a in accs]
+    big = np.ascontiguousarray(scenes.camera_rays_jittered(
+        100_000, 77, eye=np.array([0.5, 0.5, -1.5]) * SCALE, look=np.array([0.5, 0.5, 0.5]) * SCALE))
+    small = _requests(tris, 10, seed=902, max_rays=12000)
+    rid_big = srv.submit(ids[1], big, CLOSEST)
+    rids = [srv.submit(ids[s], r, k) for s, k, r in small]
+    shadow = np.ascontiguousarray(scenes.surface_rays(
+        tris[1], 50_000, 78, "shadow", light_center=LIGHT, light_size=0.1 * SCALE,
+        offset=0.01 * SCALE))
+    rid_sh = srv.submit(ids[1], shadow, ANY)
+    out, info = srv.wait(rid_big)
+    want = accs[1].intersect(big)
+    assert info["nrays"] == len(big)
+    assert np.array_equal(out["tri"], want["tri"])
+    assert np.array_equal(out["t"].view(np.int32), want["t"].view(np.int32))
+    out_sh, _ = srv.wait(rid_sh)
+    assert np.array_equal(out_sh, accs[1].occluded(shadow))
+    for (s, k, r), rid in zip(small, rids):
+        o, _ = srv.wait(rid)
+        w = accs[s].intersect(r) if k == CLOSEST else accs[s].occluded(r)
+        if k == CLOSEST:
+            assert np.array_equal(o["tri"], w["tri"])
+        else:
+            assert np.array_equal(o, w)
+    srv.destroy()
+
+
+def test_a_stopped_piece_fails_only_its_own_request(gpu):
+    """Every request has its own status: with a stack bound too shallow for
+    one scene's tree, that scene's requests report ENC_ERR_WATCHDOG while the
+    requests on a shallow scene in the same rounds finish normally."""
+    from encore_b200 import LaunchConfig
+    shallow = scenes.random_triangles(40, seed=903, scale=SCALE)
+    deep = scenes.random_triangles(200_000, seed=904, scale=SCALE)
+    a_sh, a_dp = Accelerator("wbvh").build(shallow), Accelerator("wbvh").build(deep)
+    srv = Server(slots=1, slot_rays=1 << 18, launch=LaunchConfig(stack_depth=2))
+    i_sh, i_dp = srv.add_scene(a_sh), srv.add_scene(a_dp)
+    cam = dict(eye=np.array([0.5, 0.5, -1.5]) * SCALE, look=np.array([0.5, 0.5, 0.5]) * SCALE)
+    r_sh = np.ascontiguousarray(scenes.camera_rays_jittered(5000, 905, **cam))
+    r_dp = np.ascontiguousarray(scenes.camera_rays_jittered(5000, 906, **cam))
+    rid_dp = srv.submit(i_dp, r_dp, CLOSEST)
+    rid_sh = srv.submit(i_sh, r_sh, CLOSEST)
+    with pytest.raises(EncoreError) as ei:
+        srv.wait(rid_dp)
+    assert ei.value.status == 4  # ENC_ERR_WATCHDOG
+    out, info = srv.wait(rid_sh)
+    assert info["status"] == 0
+    want = a_sh.intersect(r_sh)
+    assert np.array_equal(out["tri"], want["tri"])
+    srv.destroy()
+    a_sh.destroy()
+    a_dp.destroy()

@@ -31,6 +31,49 @@ class FakeAccel:
         return h
 
 
+class FakeServer:
+    """Stands in for a rank's serving.Server: records which scenes it holds
+    and which requests it served; a request's hits are a pure function of its
+    rays and its scene (so a request answered on the wrong scene or rank, or
+    returned out of order, is caught)."""
+
+    def __init__(self):
+        self.scenes, self.served, self._out = [], [], {}
+
+    def add_scene(self, acc):
+        self.scenes.append(acc)
+        return len(self.scenes) - 1
+
+    def submit(self, sid, rays, kind=0):
+        scene = self.scenes[sid]
+        self.served.append(scene)
+        rid = len(self.served)
+        self._out[rid] = expected_output(scene, rays, kind)
+        return rid
+
+    def wait(self, rid):
+        return self._out.pop(rid), {"status": 0}
+
+
+def expected_output(scene, rays, kind):
+    if kind == 0:
+        h = np.zeros(len(rays), HIT_DTYPE)
+        h["tri"] = np.floor(rays[:, 0] * 1000).astype(np.int32) + 100000 * scene
+        h["t"] = rays[:, 4] + rays[:, 5]
+        return h
+    return ((np.floor(rays[:, 1] * 10).astype(np.int64) + scene) % 2).astype(np.uint8)
+
+
+def routed_requests():
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(23):
+        s = int(rng.integers(0, 7))
+        n = int(rng.integers(0, 500))
+        reqs.append((s, int(rng.integers(0, 2)), rng.random((n, 8)).astype(np.float32)))
+    return reqs
+
+
 def _worker(rank, ws, port, q, case):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -69,6 +112,26 @@ def _worker(rank, ws, port, q, case):
             want = FakeAccel().intersect(rays)
             out["sharded_ok"] = bool(np.array_equal(hits, want))
         out["owners"] = replicas.route_scenes([5, 1, 4, 4, 2, 9], ws)
+        # serving by scene affinity: 7 scenes over the ranks, requests
+        # submitted on rank 0 and answered by the scenes' owners
+        srv = FakeServer()
+        router = replicas.SceneRouter([5, 1, 4, 4, 2, 9, 3], srv, build_scene=lambda s: s)
+        reqs = routed_requests() if rank == 0 else None
+        res = router.run(reqs)
+        out["router_owner"] = router.owner
+        out["router_scenes"] = sorted(srv.scenes)
+        out["router_served"] = sorted(set(srv.served))
+        if rank == 0:
+            out["router_ok"] = all(
+                np.array_equal(np.asarray(got).view(np.uint8),
+                               expected_output(s, r, k).view(np.uint8))
+                for got, (s, k, r) in zip(res, reqs))
+            out["router_n"] = len(res)
+        res2 = router.run(reqs)  # a second batch through the same router
+        if rank == 0:
+            out["router_again"] = all(np.array_equal(np.asarray(a).view(np.uint8),
+                                                     np.asarray(b).view(np.uint8))
+                                      for a, b in zip(res, res2))
         dist.barrier()
         dist.destroy_process_group()
         q.put((rank, out))
@@ -150,3 +213,18 @@ def test_rank_that_leaves_ends_the_others_collective_with_an_error():
     res = run_ranks("leave", timeout=90)
     assert res[1]["left"]
     assert res[0]["error"] is not None
+
+
+def test_scene_router_serves_each_request_on_its_owner_in_order():
+    """Multi-GPU serving by scene affinity (world size 2, gloo): both ranks
+    compute the same owners; each rank holds and serves only its own scenes;
+    the front end gets every request's result, in submission order, twice."""
+    res = run_ranks("ok")
+    assert res[0]["router_owner"] == res[1]["router_owner"]
+    owner = res[0]["router_owner"]
+    for r in (0, 1):
+        mine = [s for s, o in enumerate(owner) if o == r]
+        assert res[r]["router_scenes"] == mine
+        assert set(res[r]["router_served"]) <= set(mine)
+    assert res[0]["router_ok"] and res[0]["router_n"] == 23
+    assert res[0]["router_again"]

@@ -17,7 +17,7 @@ from oracle import bindings as ob
 from oracle import scene_port
 from tests.scene_files import mesh, write_ply, write_scene
 
-REF_MODELS = Path("/root/reference/ENCORE")
+REF_MODELS = ob.REFERENCE_DIR
 
 
 def bits(a):
