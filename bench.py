@@ -841,8 +841,23 @@ def run_engine_arm(args, rank: int, world: int) -> None:
         ms_kd, _ = timed(kd_closest, max(1, args.steps // 4))
         kd.check(stream)
         kd_rate, _ = replicas.aggregate_rate(n, len(ms_kd), sum(ms_kd))
-        kd_value = {"mrays_s": round(kd_rate / 1e6, 3), "build_seconds": round(kd_build_s, 2)}
         kd_hits = d_hits.cpu().numpy().view(np.int32)
+        # the same walk over the binned order (coherent warps), same hits
+        kd_scratch = torch.empty(kd.bin_scratch_bytes(n), dtype=torch.uint8, device=dev)
+
+        def kd_binned(mid=None):
+            if mid is not None:
+                mid.record(stream)
+            kd.intersect_device_binned(d_rays, n, d_hits, kd_scratch, stream=stream)
+
+        kd_binned()
+        ms_kdb, _ = timed(kd_binned, max(1, args.steps // 4))
+        kd.check(stream)
+        kdb_rate, _ = replicas.aggregate_rate(n, len(ms_kdb), sum(ms_kdb))
+        kd_same = bool(np.array_equal(d_hits.cpu().numpy().view(np.int32), kd_hits))
+        kd_value = {"mrays_s": round(kd_rate / 1e6, 3), "mrays_s_binned": round(kdb_rate / 1e6, 3),
+                    "binned_same_hits": kd_same, "build_seconds": round(kd_build_s, 2)}
+        del kd_scratch
         kd.destroy()
         if rank == 0:
             parity = parity_vs_kd(got, kd_hits)

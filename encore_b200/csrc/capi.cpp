@@ -544,10 +544,6 @@ enc_status enc_intersect_closest_device_ordered(enc_accel a, const float* d_rays
     set_error("enc_intersect_closest_device_ordered: too many rays in one call");
     return ENC_ERR_INVALID_ARG;
   }
-  if (a->dev.kind != ENC_ACCEL_WBVH) {
-    set_error("enc_intersect_closest_device_ordered: wide BVH only");
-    return ENC_ERR_UNSUPPORTED;
-  }
   DeviceScope ds(a->dev.device);
   Launch L = resolve_launch(launch, a->dev.kind, a->dev.width);
   if (L.block % 32 != 0 || L.block > 128 || (L.stack != 0 && L.stack < 2) || L.stack > 64 || L.chunk < 1) {
@@ -571,10 +567,6 @@ enc_status enc_intersect_closest_device_binned(enc_accel a, const float* d_rays,
   if (nrays > 0xffffffffull / 2) {
     set_error("enc_intersect_closest_device_binned: too many rays in one call");
     return ENC_ERR_INVALID_ARG;
-  }
-  if (a->dev.kind != ENC_ACCEL_WBVH) {
-    set_error("enc_intersect_closest_device_binned: wide BVH only");
-    return ENC_ERR_UNSUPPORTED;
   }
   int ob, db;
   float pf;

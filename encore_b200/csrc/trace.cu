@@ -436,11 +436,15 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             }
           }
           // triangles of the hit leaves (meta = count << 5 | offset)
+          // (the meta bytes are words 6 and 7 of the node, bytes 24-31; they
+          // are picked by select and shift, not by indexing the node array
+          // with the runtime slot c, which would move it to local memory)
           uint32_t lh = hm & ~imask;
+          const uint32_t mlo = nw.w[1].z, mhi = nw.w[1].w;
           while (lh) {
             const uint32_t c = __ffs(lh) - 1;
             lh &= lh - 1;
-            const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
+            const uint32_t meta = (((c & 4u) ? mhi : mlo) >> ((c & 3u) * 8u)) & 0xffu;
             trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
           }
           // hit internal children in octant order: bit k = slot k ^ octm
@@ -739,6 +743,7 @@ struct KdParams {
   const uint32_t* items;
   const float4* tris;  // triangle-ID order
   const float4* rays;
+  const uint32_t* order;  // null, or: the i-th ray walked is ray order[i] (binned batches)
   void* out;
   uint32_t* status;
   unsigned nrays, nnodes, nitems, ntris;
@@ -749,8 +754,13 @@ constexpr int kKdStack = 64;
 
 template <bool CLAMP, bool ANY>
 __global__ void __launch_bounds__(128) kd_trace(KdParams P) {
-  for (unsigned ray = blockIdx.x * blockDim.x + threadIdx.x; ray < P.nrays;
-       ray += gridDim.x * blockDim.x) {
+  for (unsigned qi = blockIdx.x * blockDim.x + threadIdx.x; qi < P.nrays;
+       qi += gridDim.x * blockDim.x) {
+    const unsigned ray = P.order ? __ldg(P.order + qi) : qi;
+    if (ray >= P.nrays) {  // an order entry outside the batch: skipped and reported
+      atomicOr(P.status, kStatusBounds);
+      continue;
+    }
     const float4 r0 = __ldg(P.rays + 2 * (size_t)ray);
     const float4 r1 = __ldg(P.rays + 2 * (size_t)ray + 1);
     const float o[3] = {r0.x, r0.y, r0.z};
@@ -933,12 +943,14 @@ int dispatch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32
 }
 
 template <bool ANY>
-int launch_kd(const DevAccel& a, const float* rays, size_t n, void* out, cudaStream_t s) {
+int launch_kd(const DevAccel& a, const float* rays, size_t n, void* out, cudaStream_t s,
+              const uint32_t* order = nullptr) {
   KdParams p;
   p.nodes = a.d_kd;
   p.items = a.d_kd_items;
   p.tris = reinterpret_cast<const float4*>(a.d_tris);
   p.rays = reinterpret_cast<const float4*>(rays);
+  p.order = order;
   p.out = out;
   p.status = a.d_status;
   p.nrays = (unsigned)n;
@@ -978,7 +990,7 @@ int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_
                    const Launch& L, void* stream, uint32_t* d_visits, const uint32_t* d_order) {
   if (n == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (a.kind == ENC_ACCEL_KDTREE) return launch_kd<false>(a, d_rays, n, d_hits, s);
+  if (a.kind == ENC_ACCEL_KDTREE) return launch_kd<false>(a, d_rays, n, d_hits, s, d_order);
   if (d_visits) return dispatch_w<false, true>(a, d_rays, n, d_hits, d_visits, L, s, d_order);
   return dispatch_w<false, false>(a, d_rays, n, d_hits, nullptr, L, s, d_order);
 }

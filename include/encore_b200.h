@@ -223,7 +223,9 @@ enc_status enc_intersect_closest_device(enc_accel accel, const float* d_rays, si
  * d_scratch: device memory of at least enc_bin_scratch_bytes() bytes,
  * 256-byte aligned, owned by the caller and used on `stream` only until the
  * launch completes (calls that share one scratch buffer must be ordered on
- * one stream).  No counterpart in the reference (one ray per call). */
+ * one stream).  Both accelerator kinds: the kd-tree parity mode, which
+ * walks one ray per thread, gains most from coherent warps.  No counterpart
+ * in the reference (one ray per call). */
 typedef struct enc_bin_opts {
   int32_t origin_bits;
   int32_t dir_bits;

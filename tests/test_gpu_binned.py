@@ -93,11 +93,17 @@ def test_binned_argument_errors(gpu, field):
         acc.intersect_device_binned(d_rays, n, d_hits, big[16:])
     with pytest.raises(EncoreError):  # more than 20 key bits
         acc.bin_scratch_bytes(n, BinConfig(16, 8))
-    kd = Accelerator("kdtree").build(tris[:200])
-    with pytest.raises(EncoreError):
-        kd.intersect_device_binned(d_rays, n, d_hits, big)
-    kd.destroy()
     acc.intersect_device_binned(d_rays, 0, d_hits, big)  # empty batch: nothing to do
+
+
+def test_binned_kd_parity_mode_is_unchanged(gpu, field):
+    """The kd-tree parity mode walks the binned order too; every hit is the
+    unbinned walk's (and so the reference Kdtree's) bit for bit."""
+    tris, rays, acc = field
+    kd = Accelerator("kdtree").build(tris)
+    plain, binned = _dev_hits(kd, rays)
+    assert np.array_equal(plain, binned)
+    kd.destroy()
 
 
 def test_bin_then_ordered_trace_equals_plain(gpu, field):
