@@ -11,13 +11,13 @@ Workload (one step = one pass of the closest-hit kernel over one batch):
   also   as many any-hit shadow rays toward a 0.1 x 0.1 light at height 2.0
          (reported as anyhit_mrays_s).
 
-value: Mrays/s with rays and hits resident in HBM; one step = the binning
-pass (enc_bin_rays: a counting sort of the batch by origin and direction
-cell) + the closest-hit launch over the binned order
-(enc_intersect_closest_device_ordered), both inside the timed region;
-timed with CUDA events on the launch stream, L2 flushed (256 MiB write)
-between timed steps; max over ranks; whole-job aggregate.  --no-bin times
-the unbinned launch instead.  e2e: the same metric through the host-buffer
+value: Mrays/s with rays and hits resident in HBM; one step = one
+closest-hit launch over the batch (enc_intersect_closest_device); timed
+with CUDA events on the launch stream, L2 flushed (256 MiB write) between
+timed steps; max over ranks; whole-job aggregate.  --bin adds the binning
+pass (enc_bin_rays, a counting sort of the batch by origin and direction
+cell) to every step and traces the binned order
+(enc_intersect_closest_device_ordered).  e2e: the same metric through the host-buffer
 C-ABI call (enc_intersect_closest) from pinned host memory, copies inside
 the timed region.  --gpus N runs N independent replicas (one process per
 GPU, each with its own seeded batch, no collective on the data path).
@@ -751,7 +751,7 @@ def run_engine_arm(args, rank: int, world: int) -> None:
     d_shadow = torch.from_numpy(shadow).to(dev)
     d_occ = torch.empty(n, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    binning = None if args.no_bin else BinConfig(args.bin_origin, args.bin_dir, args.bin_probe)
+    binning = BinConfig(args.bin_origin, args.bin_dir, args.bin_probe) if args.bin else None
     scratch = (torch.empty(acc.bin_scratch_bytes(n, binning), dtype=torch.uint8, device=dev)
                if binning else None)
 
@@ -988,8 +988,9 @@ def main():
     ap.add_argument("--bps", type=int, default=0)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--stack", type=int, default=0)
-    ap.add_argument("--no-bin", action="store_true",
-                    help="time the unbinned closest-hit launch (no binning pass)")
+    ap.add_argument("--bin", action="store_true",
+                    help="bin the batch (enc_bin_rays) inside every step and trace it in that "
+                         "order (measured slower than the plain launch on this workload)")
     ap.add_argument("--bin-origin", type=int, default=0, help="binning key: origin bits (0 = default)")
     ap.add_argument("--bin-dir", type=int, default=0, help="binning key: direction bits")
     ap.add_argument("--bin-probe", type=float, default=0.0,

@@ -218,8 +218,19 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherParams P) {
           if (lane == 0) atomicOr(P.status, 2u);
           break;
         }
+        // Nearest child on top: the passing children are pushed farthest
+        // first, so the walk visits them nearest first, the heap fills with
+        // nearer photons and its maximum (the search radius once full)
+        // shrinks sooner.  A child's place = the passing children farther
+        // than it (equal distances: the higher lane counts as farther).
+        int farther = 0;
+        for (unsigned mm = m; mm; mm &= mm - 1u) {
+          const int j = __ffs(mm) - 1;
+          const float dj = __shfl_sync(kFull, cd, j);
+          farther += (dj > cd || (dj == cd && j > (int)lane)) ? 1 : 0;
+        }
         if (pass) {
-          const int at = sp + __popc(m & lt);
+          const int at = sp + farther;
           uint32_t item = ((uint32_t)cl << 28) | child;
           uint32_t cnt = 0;
           if (cl == 0) {  // a leaf: its photon range goes onto the stack

@@ -214,7 +214,12 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
   __shared__ uint32_t s_coop_own[kCoop ? 128 : 1];
   __shared__ unsigned long long s_coop_key[kCoop ? 128 : 1];
   __shared__ float2 s_coop_uv[kCoop ? 128 : 1];
-  __shared__ float4 s_ray[kCoop ? 256 : 1];  // each lane's ray, for the rounds' workers
+  // Each lane's ray, its reciprocal direction and sign bits, stored when the
+  // lane takes the ray: the rounds' workers read their owners' rays here, and
+  // with kRayShared the lane itself rereads them at every node instead of
+  // holding eleven registers across the traversal loop.
+  constexpr bool kRayShared = kCoop;
+  __shared__ float4 s_ray[kCoop ? 384 : 1];
   const int B = blockDim.x;
   uint2* stk = s_stack + threadIdx.x;  // entry i at stk[i * B]
   float* slb = reinterpret_cast<float*>(s_stack + (size_t)P.stack_depth * B) + threadIdx.x;
@@ -315,10 +320,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         const float4 r1 = __ldg(rp + 1);
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
-        if (kCoop) {
-          s_ray[2 * threadIdx.x] = r0;
-          s_ray[2 * threadIdx.x + 1] = r1;
-        }
+
         // Box tests use a reciprocal with |d| floored at 1e-20 so that a zero
         // direction component (the reference's Normalize clamps small ones to
         // exactly 0) gives finite slab distances instead of 0 * inf = NaN,
@@ -338,6 +340,11 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         iy = rcp(fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy));
         iz = rcp(fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz));
         octm = (dx < 0.f ? 1u : 0u) | (dy < 0.f ? 2u : 0u) | (dz < 0.f ? 4u : 0u);
+        if (kCoop) {
+          s_ray[3 * threadIdx.x] = r0;
+          s_ray[3 * threadIdx.x + 1] = r1;
+          s_ray[3 * threadIdx.x + 2] = make_float4(ix, iy, iz, __uint_as_float(octm));
+        }
         best_t = tmax; best_id = -1; bu = 0.f; bv = 0.f;
         sp = 0;
         node = 0;  // root
@@ -380,16 +387,24 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
         const uint32_t child_base = nw.w[1].x;
         const uint32_t tri_base = nw.w[1].y;
-        const float bx = (px - ox) * ix, by = (py - oy) * iy, bz = (pz - oz) * iz;
-        const float cx = sx * ix, cy = sy * iy, cz = sz * iz;
+        float vox = ox, voy = oy, voz = oz, vtmin = tmin, vix = ix, viy = iy, viz = iz;
+        uint32_t voct = octm;
+        if constexpr (kRayShared) {
+          const float4 sa = s_ray[3 * threadIdx.x], sc = s_ray[3 * threadIdx.x + 2];
+          vox = sa.x; voy = sa.y; voz = sa.z; vtmin = sa.w;
+          vix = sc.x; viy = sc.y; viz = sc.z;
+          voct = __float_as_uint(sc.w);
+        }
+        const float bx = (px - vox) * vix, by = (py - voy) * viy, bz = (pz - voz) * viz;
+        const float cx = sx * vix, cy = sy * viy, cz = sz * viz;
         // Near and far planes per axis by the ray's direction sign: the
         // near plane of a child box is its lo corner for a positive
         // direction and its hi corner for a negative one.
-        const bool nxs = (octm & 1u) != 0, nys = (octm & 2u) != 0, nzs = (octm & 4u) != 0;
+        const bool nxs = (voct & 1u) != 0, nys = (voct & 2u) != 0, nzs = (voct & 4u) != 0;
         float key[W];
         uint32_t rnk[W];
         uint32_t trimask = 0;
-        uint32_t hitk = 0;      // W == 8: hit internal children, bit k = slot k ^ octm
+        uint32_t hitk = 0;      // W == 8: hit internal children, bit k = slot k ^ voct
         float lbmin = INFINITY;  // W == 8: smallest entry distance of those
         int nh = 0;
         // Width 8: the six plane arrays are whole words (qlo x at words 8-9,
@@ -427,7 +442,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             const float tnz = fmaf(__uint_as_float(__byte_perm(wn[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
             const float tfz = fmaf(__uint_as_float(__byte_perm(wf[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
             // (three-input min/max measured 1.6 % slower here)
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, vtmin));
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
             if (tn <= tf) {
               hm |= 1u << c;
@@ -447,11 +462,11 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             const uint32_t meta = (((c & 4u) ? mhi : mlo) >> ((c & 3u) * 8u)) & 0xffu;
             trimask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
           }
-          // hit internal children in octant order: bit k = slot k ^ octm
+          // hit internal children in octant order: bit k = slot k ^ voct
           uint32_t x = hm & imask;
-          if (octm & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
-          if (octm & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
-          if (octm & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
+          if (voct & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
+          if (voct & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
+          if (voct & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
           hitk = x;
         } else {
 #pragma unroll
@@ -468,7 +483,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
             const float tfy = fmaf(u8f(nys ? qly : qhy), cy, by);
             const float tnz = fmaf(u8f(nzs ? qhz : qlz), cz, bz);
             const float tfz = fmaf(u8f(nzs ? qlz : qhz), cz, bz);
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, vtmin));
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
             const uint32_t meta = byte_of(nw.w, L::kMetaOff + c);
             const bool hit = meta != 0u && tn <= tf;
@@ -485,7 +500,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
           if (hitk) {
             const uint32_t imask = ew >> 24;
             const uint32_t k = __ffs(hitk) - 1;
-            const uint32_t slot = k ^ octm;
+            const uint32_t slot = k ^ voct;
             node = child_base + __popc(imask & ((1u << slot) - 1u));
             const uint32_t rest = hitk & (hitk - 1u);
             if (rest) {
@@ -535,7 +550,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         tmask = trimask;
         tbase = tri_base;
         if (kCoop) trimask = 0;  // tested below by the whole warp
-        while (trimask) {
+        while (!kCoop && trimask) {
           const uint32_t k = __ffs(trimask) - 1;
           trimask &= trimask - 1;
           const uint32_t ti = tri_base + k;
@@ -607,7 +622,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
         const int own = (int)lane < nitems ? (int)it_own[lane] : (int)lane;
         // the owner's ray, kept in shared memory since its refill (two
         // 16-byte loads instead of seven shuffles; measured +1 %)
-        const float4 wr0 = s_ray[2 * (wib * 32 + own)], wr1 = s_ray[2 * (wib * 32 + own) + 1];
+        const float4 wr0 = s_ray[3 * (wib * 32 + own)], wr1 = s_ray[3 * (wib * 32 + own) + 1];
         const float wox = wr0.x, woy = wr0.y, woz = wr0.z, wtmin = wr0.w;
         const float wdx = wr1.x, wdy = wr1.y, wdz = wr1.z;
         const float wlim = __shfl_sync(kFull, ANY ? tmax : best_t, own);
@@ -689,7 +704,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClose
           if constexpr (W == 8) {
             const uint32_t hk = e.y & 0xffu;
             const uint32_t k = __ffs(hk) - 1;
-            const uint32_t slot = k ^ octm;
+            const uint32_t slot =
+                k ^ (kRayShared ? __float_as_uint(s_ray[3 * threadIdx.x + 2].w) : octm);
             const uint32_t imask = (e.y >> 8) & 0xffu;
             node = e.x + __popc(imask & ((1u << slot) - 1u));
             const uint32_t rest = hk & (hk - 1u);

@@ -47,6 +47,12 @@ def port():
         lib.eo_kd_closest.argtypes = [P, P, C.c_long, C.c_int, P, C.c_int]
         lib.eo_kd_free.argtypes = [P]
         lib.eo_kd_tested.argtypes = [P, P, P, C.c_long, C.c_int, P, C.c_int]
+        lib.eo_kd_leaves_at.argtypes = [P, P, C.c_float, P, C.c_int]
+        lib.eo_kd_leaves_at.restype = C.c_int
+        lib.eo_kd_leaf_has.argtypes = [P, C.c_int32, C.c_int32]
+        lib.eo_kd_leaf_has.restype = C.c_int
+        lib.eo_kd_walk.argtypes = [P, P, C.c_int, P, P, P, C.c_int]
+        lib.eo_kd_walk.restype = C.c_int
         lib.eo_pmap_build.restype = P
         lib.eo_pmap_build.argtypes = [P, P, P, C.c_long]
         lib.eo_pmap_gather.argtypes = [P, P, P, C.c_long, C.c_int, C.c_float, C.c_int, C.c_int,
@@ -156,7 +162,7 @@ def share_vertex(tris, a, b):
 
 
 CLASS_NAMES = ("tie", "edge", "want_false_positive", "got_false_positive", "grazing",
-               "closer_untested", "unexplained")
+               "closer_untested", "unexplained", "split_plane_nan")
 
 
 def classify(tris, rays, got, want, kd=None):
@@ -170,6 +176,13 @@ def classify(tris, rays, got, want, kd=None):
     'want_false_positive' / 'got_false_positive'  that side's triangle is not
             hit geometrically in FP64 (a Cross() clamp artefact);
     'grazing'  |t_got - t_want| <= 1e-5 relative, both geometric;
+    'split_plane_nan'  (only with kd): as closer_untested, for a ray whose
+            origin lies exactly on a kd split plane and whose direction has
+            an exactly zero component (the reference's Normalize snaps
+            components below 0.001 to 0, H2): along that axis
+            Kdtree::intersect forms tplane = (split - o) * (1 / 0) = 0 * inf
+            = NaN (Kdtree.cpp:712), and its walk's [tmin, tmax] bookkeeping
+            passes over the cells that hold the hit;
     'closer_untested'  (only with kd = the reference's kd walk, a PortKd):
             got's hit is geometric in FP64 and closer than want's (or want
             misses), and the kd walk never tests got's triangle -- its cells
@@ -207,7 +220,9 @@ def classify(tris, rays, got, want, kd=None):
             classes.append("grazing")
         elif (kd is not None and g_id >= 0 and gh[j] and (w_id < 0 or tg < tw)
               and untested[j]):
-            classes.append("closer_untested")
+            rr = r[j]
+            in_plane = bool(np.any(rr[4:7] == 0)) and len(kd.leaves_at(rr[0:3], 0.0)) > 1
+            classes.append("split_plane_nan" if in_plane else "closer_untested")
         else:
             classes.append("unexplained")
     return mism, classes
@@ -228,6 +243,26 @@ class PortKd:
         self.lib.eo_kd_closest(self.h, rays.ctypes.data, rays.shape[0], int(clamp),
                                out.ctypes.data, nthreads)
         return out
+
+    def leaves_at(self, p, eps=0.0):
+        """Leaves whose cells contain point p (both sides of a split within eps)."""
+        pt = np.ascontiguousarray(p, np.float32)
+        out = np.empty(256, np.int32)
+        n = self.lib.eo_kd_leaves_at(self.h, pt.ctypes.data, float(eps), out.ctypes.data, 256)
+        return out[:n]
+
+    def leaf_has(self, leaf, tri_id):
+        return bool(self.lib.eo_kd_leaf_has(self.h, int(leaf), int(tri_id)))
+
+    def walk(self, ray, clamp=True, max_leaves=4096):
+        """The leaves one ray's reference walk visits: (leaves, tmin, tmax)."""
+        r = np.ascontiguousarray(ray, np.float32)
+        lv = np.empty(max_leaves, np.int32)
+        t0 = np.empty(max_leaves, np.float32)
+        t1 = np.empty(max_leaves, np.float32)
+        n = self.lib.eo_kd_walk(self.h, r.ctypes.data, int(clamp), lv.ctypes.data,
+                                t0.ctypes.data, t1.ctypes.data, max_leaves)
+        return lv[:n], t0[:n], t1[:n]
 
     def tested(self, rays, ids, clamp=True, nthreads=0):
         """Per ray: does the reference kd walk test triangle ids[i] at all?"""

@@ -1062,3 +1062,123 @@ int eo_photon_trace(const float* tris, int ntris, const eo_photon_opts* o, int c
   free(c.count);
   return c.shadow_dropped ? 1 : 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* kd walk inspection (explains rays the reference walk passes over)         */
+
+/* The leaves whose cells contain point p: descend by the node's split
+ * (read as Kdtree::intersect reads it, snapped to 0 within 0.001), both
+ * children where |p - split| <= eps.  Returns the number written (<= max). */
+int eo_kd_leaves_at(void* p_kd, const float* p, float eps, int32_t* leaves, int max) {
+  const kdtree* kd = (const kdtree*)p_kd;
+  uint32_t stack[256];
+  int sp = 0, n = 0;
+  stack[sp++] = 0;
+  while (sp > 0 && n < max) {
+    const uint32_t node = stack[--sp];
+    const kdnode nd = kd->nodes[node];
+    if ((nd.w0 & 3u) == 3u) {
+      leaves[n++] = (int32_t)node;
+      continue;
+    }
+    const int axis = (int)(nd.w0 & 3u);
+    float split;
+    memcpy(&split, &nd.w0, 4);
+    split = (split > -0.001 && split < 0.001) ? 0 : split;
+    const float d = p[axis] - split;
+    if (d <= eps && sp < 255) stack[sp++] = nd.w1;
+    if (d >= -eps && sp < 255) stack[sp++] = nd.w1 + 1;
+  }
+  return n;
+}
+
+/* 1 if triangle id is in leaf `leaf`'s item list. */
+int eo_kd_leaf_has(void* p_kd, int32_t leaf, int32_t id) {
+  const kdtree* kd = (const kdtree*)p_kd;
+  const kdnode nd = kd->nodes[leaf];
+  if ((nd.w0 & 3u) != 3u) return 0;
+  const uint32_t cnt = nd.w0 >> 2;
+  for (uint32_t k = 0; k < cnt; ++k)
+    if ((int32_t)kd->items[nd.w1 + k] == id) return 1;
+  return 0;
+}
+
+/* The reference walk of one ray (kd_closest_range's steps): the leaves it
+ * visits in order with their [tmin, tmax]; returns the count (<= max). */
+int eo_kd_walk(void* p_kd, const float* r, int clamp, int32_t* leaves, float* tmins,
+               float* tmaxs, int max) {
+  const kdtree* kd = (const kdtree*)p_kd;
+  const float o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
+  const float inv[3] = {1.f / d[0], 1.f / d[1], 1.f / d[2]};
+  float best = INFINITY;
+  float t0 = 0, t1 = INFINITY;
+  for (int a = 0; a < 3; ++a) {
+    float tin = (kd->root_lo[a] - o[a]) / d[a];
+    float tout = (kd->root_hi[a] - o[a]) / d[a];
+    if (tin > tout) {
+      float tt = tin;
+      tin = tout;
+      tout = tt;
+    }
+    t0 = tin > t0 ? tin : t0;
+    t1 = tout < t1 ? tout : t1;
+    if (t0 > t1) return 0;
+  }
+  float tmin = t0, tmax = t1;
+  uint32_t sn[128];
+  float smin[128], smax[128];
+  int sp = 0, n = 0;
+  uint32_t node = 0;
+  for (;;) {
+    if (best < tmin) break;
+    kdnode nd = kd->nodes[node];
+    if ((nd.w0 & 3u) != 3u) {
+      int axis = (int)(nd.w0 & 3u);
+      float split;
+      memcpy(&split, &nd.w0, 4);
+      split = (split > -0.001 && split < 0.001) ? 0 : split;
+      float tplane = (split - o[axis]) * inv[axis];
+      int below = o[axis] <= split;
+      uint32_t first = below ? nd.w1 : nd.w1 + 1;
+      uint32_t second = below ? nd.w1 + 1 : nd.w1;
+      if (tplane == 0) {
+        node = inv[axis] > 0 ? second : first;
+      } else if (tplane >= tmax || tplane < 0) {
+        node = first;
+      } else if (tplane <= tmin) {
+        node = second;
+      } else {
+        if (sp < 128) {
+          sn[sp] = second;
+          smin[sp] = tplane;
+          smax[sp] = tmax;
+          ++sp;
+        }
+        node = first;
+        tmax = tplane;
+      }
+    } else {
+      if (n < max) {
+        leaves[n] = (int32_t)node;
+        tmins[n] = tmin;
+        tmaxs[n] = tmax;
+        ++n;
+      }
+      uint32_t cnt = nd.w0 >> 2;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        uint32_t id = kd->items[nd.w1 + k];
+        float t, a, bt;
+        if (eo_tri_test(kd->tris + 9 * (size_t)id, r, clamp, &t, &a, &bt) && t < best) best = t;
+      }
+      if (sp > 0) {
+        --sp;
+        node = sn[sp];
+        tmin = smin[sp];
+        tmax = smax[sp];
+      } else {
+        break;
+      }
+    }
+  }
+  return n;
+}

@@ -62,6 +62,13 @@ void eo_kd_free(void* kd);
  * (ids[i] < 0: never).  Used to explain a closer hit the walk passed over. */
 void eo_kd_tested(void* kd, const float* rays, const int32_t* ids, long n, int clamp,
                   uint8_t* tested, int nthreads);
+/* Inspection of the walk: the leaves whose cells contain a point (both sides
+ * of a split within eps), whether a leaf lists a triangle, and the leaves one
+ * ray's walk visits with their [tmin, tmax]. */
+int eo_kd_leaves_at(void* kd, const float* p, float eps, int32_t* leaves, int max);
+int eo_kd_leaf_has(void* kd, int32_t leaf, int32_t id);
+int eo_kd_walk(void* kd, const float* ray8, int clamp, int32_t* leaves, float* tmins,
+               float* tmaxs, int max);
 
 /* Photon gather: the k nearest accepted photons within max_dist
  * (PhotonMap::GetNearestNPhotons, PhotonMap.cpp:76-94, 224-297: accept

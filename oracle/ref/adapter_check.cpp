@@ -302,7 +302,8 @@ int main() {
   std::printf("emit status %d direct %d indirect %d emitted %u abi %u %u %u\n", (int)es,
               direct.GetCountStored(), indirect.GetCountStored(), emitted, stored[0], stored[1],
               emitted2);
-  ok &= es == ENC_OK && es2 == ENC_OK && indirect.Full() && emitted > po.nphotons &&
+  ok &= es == ENC_OK && es2 == ENC_OK && indirect.Full() && emitted >= po.nphotons &&
+        emitted % po.nphotons == 0 &&
         emitted == emitted2 && (uint32_t)direct.GetCountStored() == stored[0] &&
         (uint32_t)indirect.GetCountStored() == stored[1] && stored[0] > 0;
   std::printf("result %s\n", ok ? "pass" : "fail");
