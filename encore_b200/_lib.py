@@ -138,6 +138,8 @@ SIGNATURES = {
     "enc_accel_build": (C.c_int32, [P, C.POINTER(BuildOpts), C.c_int32, C.POINTER(P)]),
     "enc_accel_destroy": (C.c_int32, [P]),
     "enc_accel_refit": (C.c_int32, [P, P, C.c_uint32]),
+    "enc_accel_serialize": (C.c_int32, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "enc_accel_deserialize": (C.c_int32, [P, C.c_size_t, C.c_int32, C.POINTER(P)]),
     "enc_accel_info_get": (C.c_int32, [P, C.POINTER(AccelInfo)]),
     "enc_intersect_closest": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),

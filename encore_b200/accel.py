@@ -116,6 +116,35 @@ class Accelerator:
         check(self.lib.enc_accel_refit(self.handle, ptr(t), t.shape[0]), "enc_accel_refit")
         return self
 
+    def save(self) -> bytes:
+        """The accelerator as a byte image (enc_accel_serialize)."""
+        size = C.c_size_t()
+        check(self.lib.enc_accel_serialize(self.handle, None, 0, C.byref(size)),
+              "enc_accel_serialize")
+        buf = np.empty(size.value, np.uint8)
+        check(self.lib.enc_accel_serialize(self.handle, ptr(buf), size.value, C.byref(size)),
+              "enc_accel_serialize")
+        return buf.tobytes()
+
+    @classmethod
+    def load(cls, image: bytes, device: int = 0) -> "Accelerator":
+        """An accelerator from a byte image saved by save(), uploaded to
+        `device` without a host build (enc_accel_deserialize)."""
+        acc = cls.__new__(cls)
+        acc.lib = _lib.load()
+        acc.device = device
+        acc.handle = None
+        buf = np.frombuffer(image, dtype=np.uint8)
+        h = C.c_void_p()
+        check(acc.lib.enc_accel_deserialize(ptr(buf), buf.size, device, C.byref(h)),
+              "enc_accel_deserialize")
+        acc.handle = h
+        info = acc.info()
+        acc.kind = "wbvh" if info["kind"] == _lib.ENC_ACCEL_WBVH else "kdtree"
+        acc.ntris = info["ntris"]
+        acc.opts = _lib.BuildOpts(info["kind"], info["width"], 0, info["predicate"])
+        return acc
+
     def info(self) -> dict:
         i = _lib.AccelInfo()
         check(self.lib.enc_accel_info_get(self.handle, C.byref(i)), "enc_accel_info_get")

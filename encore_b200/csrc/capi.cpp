@@ -406,6 +406,212 @@ enc_status enc_accel_refit(enc_accel a, const float* tri_verts, uint32_t ntris) 
   return ENC_OK;
 }
 
+namespace {
+
+// Serialised accelerator: a fixed header, then the sections it sizes.
+struct AccelFileHeader {
+  char magic[8];
+  uint32_t version;
+  int32_t kind, width, predicate;
+  uint32_t ntris, nnodes, depth, kd_nitems;
+  float lo[3], hi[3], kd_lo[3], kd_hi[3];
+  uint64_t node_bytes, tri_bytes, order_bytes, items_bytes;
+};
+constexpr char kAccelMagic[8] = {'E', 'N', 'C', 'A', 'C', 'C', '0', '1'};
+constexpr uint32_t kAccelVersion = 1;
+
+size_t wbvh_node_bytes(int width) {
+  return width == 2 ? WNodeLayout<2>::kBytes : width == 4 ? WNodeLayout<4>::kBytes
+                                                          : WNodeLayout<8>::kBytes;
+}
+
+}  // namespace
+
+enc_status enc_accel_serialize(enc_accel a, void* buf, size_t cap, size_t* size) {
+  if (!a || !size) {
+    set_error("enc_accel_serialize: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const DevAccel& d = a->dev;
+  AccelFileHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kAccelMagic, 8);
+  h.version = kAccelVersion;
+  h.kind = d.kind;
+  h.width = d.width;
+  h.predicate = d.predicate;
+  h.ntris = d.ntris;
+  h.nnodes = d.nnodes;
+  h.depth = (uint32_t)d.tree_depth;
+  h.kd_nitems = d.kd_nitems;
+  for (int i = 0; i < 3; ++i) {
+    h.lo[i] = d.lo[i];
+    h.hi[i] = d.hi[i];
+    h.kd_lo[i] = d.kd_root_lo[i];
+    h.kd_hi[i] = d.kd_root_hi[i];
+  }
+  if (d.kind == ENC_ACCEL_WBVH) {
+    h.node_bytes = (uint64_t)d.nnodes * wbvh_node_bytes(d.width);
+    h.order_bytes = (uint64_t)a->host.tri_order.size() * 4;
+  } else {
+    h.node_bytes = (uint64_t)d.nnodes * sizeof(KdNode);
+    h.items_bytes = (uint64_t)d.kd_nitems * 4;
+  }
+  h.tri_bytes = (uint64_t)d.ntris * sizeof(DevTri);
+  const size_t total = sizeof(h) + h.node_bytes + h.tri_bytes + h.order_bytes + h.items_bytes;
+  *size = total;
+  if (!buf) return ENC_OK;  // size query
+  if (cap < total) {
+    set_error("enc_accel_serialize: buffer smaller than the size the call reports");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(a->mu);
+  DeviceScope ds(d.device);
+  char* p = static_cast<char*>(buf);
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  if (d.kind == ENC_ACCEL_WBVH) {
+    ENC_CUDA(cudaMemcpy(p, d.d_nodes, h.node_bytes, cudaMemcpyDeviceToHost), "read nodes");
+  } else {
+    ENC_CUDA(cudaMemcpy(p, d.d_kd, h.node_bytes, cudaMemcpyDeviceToHost), "read kd nodes");
+  }
+  p += h.node_bytes;
+  ENC_CUDA(cudaMemcpy(p, d.d_tris, h.tri_bytes, cudaMemcpyDeviceToHost), "read triangles");
+  p += h.tri_bytes;
+  if (h.order_bytes) std::memcpy(p, a->host.tri_order.data(), h.order_bytes);
+  p += h.order_bytes;
+  if (h.items_bytes)
+    ENC_CUDA(cudaMemcpy(p, d.d_kd_items, h.items_bytes, cudaMemcpyDeviceToHost), "read kd items");
+  return ENC_OK;
+}
+
+enc_status enc_accel_deserialize(const void* buf, size_t size, int32_t device, enc_accel* out) {
+  if (!buf || !out) {
+    set_error("enc_accel_deserialize: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  AccelFileHeader h;
+  if (size < sizeof(h)) {
+    set_error("enc_accel_deserialize: shorter than the header");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, kAccelMagic, 8) != 0 || h.version != kAccelVersion) {
+    set_error("enc_accel_deserialize: not a serialised accelerator of this version");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const bool wbvh = h.kind == ENC_ACCEL_WBVH;
+  if ((h.kind != ENC_ACCEL_WBVH && h.kind != ENC_ACCEL_KDTREE) ||
+      (wbvh && h.width != 2 && h.width != 4 && h.width != 8) ||
+      (h.predicate != ENC_PRED_REFERENCE && h.predicate != ENC_PRED_NOCLAMP) || h.ntris == 0 ||
+      h.nnodes == 0 || h.depth > 64 ||
+      h.node_bytes != (uint64_t)h.nnodes * (wbvh ? wbvh_node_bytes(h.width) : sizeof(KdNode)) ||
+      h.tri_bytes != (uint64_t)h.ntris * sizeof(DevTri) ||
+      h.order_bytes != (wbvh ? (uint64_t)h.ntris * 4 : 0) ||
+      h.items_bytes != (wbvh ? 0 : (uint64_t)h.kd_nitems * 4) ||
+      size != sizeof(h) + h.node_bytes + h.tri_bytes + h.order_bytes + h.items_bytes) {
+    set_error("enc_accel_deserialize: header and sizes do not agree");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const char* p = static_cast<const char*>(buf) + sizeof(h);
+  const char* nodes = p;
+  const DevTri* tris = reinterpret_cast<const DevTri*>(p + h.node_bytes);
+  const char* sec3 = p + h.node_bytes + h.tri_bytes;
+  std::vector<uint32_t> order;
+  if (wbvh) {
+    order.resize(h.ntris);
+    std::memcpy(order.data(), sec3, h.order_bytes);
+    std::vector<uint8_t> seen(h.ntris, 0);
+    for (uint32_t v : order) {
+      if (v >= h.ntris || seen[v]) {
+        set_error("enc_accel_deserialize: the triangle order is not a permutation");
+        return ENC_ERR_INVALID_ARG;
+      }
+      seen[v] = 1;
+    }
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    set_error("enc_accel_deserialize: no such CUDA device");
+    return ENC_ERR_INVALID_ARG;
+  }
+  DeviceScope ds(device);
+  if (!ds.ok) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+  enc_accel a = new (std::nothrow) enc_accel_s();
+  if (!a) return ENC_ERR_OUT_OF_MEMORY;
+  DevAccel& d = a->dev;
+  d.kind = h.kind;
+  d.width = wbvh ? h.width : 8;
+  d.predicate = h.predicate;
+  d.ntris = h.ntris;
+  d.nnodes = h.nnodes;
+  d.tree_depth = (int)h.depth;
+  d.kd_nitems = h.kd_nitems;
+  d.device = device;
+  for (int i = 0; i < 3; ++i) {
+    d.lo[i] = h.lo[i];
+    d.hi[i] = h.hi[i];
+    d.kd_root_lo[i] = h.kd_lo[i];
+    d.kd_root_hi[i] = h.kd_hi[i];
+  }
+  const double t0 = now_s();
+  cudaError_t e = cudaSuccess;
+  try {
+    if (wbvh) {
+      WBVHHost& hh = a->host;
+      hh.width = h.width;
+      hh.nnodes = h.nnodes;
+      hh.depth = (int)h.depth;
+      hh.nodes.assign(nodes, nodes + h.node_bytes);
+      hh.tri_order = order;
+      hh.tri_pos.assign(h.ntris, 0);
+      for (uint32_t i = 0; i < h.ntris; ++i) hh.tri_pos[order[i]] = i;
+      for (int i = 0; i < 3; ++i) {
+        hh.lo[i] = h.lo[i];
+        hh.hi[i] = h.hi[i];
+      }
+      uint8_t* dn = nullptr;
+      e = upload(&dn, hh.nodes.data(), hh.nodes.size());
+      d.d_nodes = dn;
+      if (e == cudaSuccess) e = upload(&d.d_tris, tris, h.ntris);
+      if (e == cudaSuccess) e = upload(&d.d_tri_pos, hh.tri_pos.data(), hh.tri_pos.size());
+    } else {
+      e = upload(&d.d_kd, reinterpret_cast<const KdNode*>(nodes), h.nnodes);
+      if (e == cudaSuccess && h.kd_nitems)
+        e = upload(&d.d_kd_items, reinterpret_cast<const uint32_t*>(sec3), h.kd_nitems);
+      if (e == cudaSuccess) e = upload(&d.d_tris, tris, h.ntris);
+    }
+  } catch (const std::bad_alloc&) {
+    free_dev(d);
+    delete a;
+    set_error("enc_accel_deserialize: host out of memory");
+    return ENC_ERR_OUT_OF_MEMORY;
+  }
+  d.node_bytes = wbvh ? h.node_bytes : h.node_bytes + h.items_bytes;
+  d.tri_bytes = h.tri_bytes;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
+  if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, kQueueSlots * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(d.d_counter, 0, kQueueSlots * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    free_dev(d);
+    delete a;
+    return cuda_fail(e, "enc_accel_deserialize: upload");
+  }
+  d.device_bytes = d.node_bytes + d.tri_bytes + (d.d_tri_pos ? 4ull * d.ntris : 0) +
+                   kQueueSlots * sizeof(uint32_t) + 16;
+  const int pe = noalloc_prepare(d);
+  if (pe != 0) {
+    free_dev(d);
+    delete a;
+    return cuda_fail((cudaError_t)pe, "enc_accel_deserialize: fixed query scratch");
+  }
+  d.build_seconds = now_s() - t0;
+  *out = a;
+  return ENC_OK;
+}
+
 enc_status enc_accel_destroy(enc_accel a) {
   if (!a) return ENC_OK;
   DeviceScope ds(a->dev.device);

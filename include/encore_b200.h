@@ -192,6 +192,19 @@ enc_status enc_accel_destroy(enc_accel accel);
 enc_status enc_accel_refit(enc_accel accel, const float* tri_verts, uint32_t ntris);
 enc_status enc_accel_info_get(enc_accel accel, enc_accel_info* info);
 
+/* Saving a built accelerator and loading it again without the host build
+ * (the reference rebuilds its trees on every run, PhotonMapperCPU.cpp:222-255;
+ * a 2M-triangle wide BVH takes over a second to build, a load only its
+ * upload).  enc_accel_serialize writes a self-contained byte image (header,
+ * nodes, triangle records, leaf order or kd item lists) into `buf`; with
+ * buf = NULL it only sets *size.  enc_accel_deserialize checks the header
+ * and every section size (ENC_ERR_INVALID_ARG on any mismatch) and uploads
+ * the image to `device`; the result answers every query exactly as the saved
+ * accelerator did and can be refitted.  The image is host-endian and tied to
+ * this library's layout version. */
+enc_status enc_accel_serialize(enc_accel accel, void* buf, size_t cap, size_t* size);
+enc_status enc_accel_deserialize(const void* buf, size_t size, int32_t device, enc_accel* out);
+
 /* AccelerationStructure::intersect (AccelerationStructure.h:63), batched.
  * Host-buffer form: copies rays in, traces, copies hits out, synchronises
  * `stream` before returning. */

@@ -44,3 +44,24 @@ def test_errors_without_device_are_reported_not_raised():
     assert b"no triangles" in lib.enc_last_error()
     lib.enc_scene_destroy(s)
     assert lib.enc_accel_build(None, None, 0, C.byref(a)) == _lib.ENC_ERR_INVALID_ARG
+
+
+def test_deserialize_rejects_malformed_images_before_any_device_call():
+    """enc_accel_deserialize checks the header and every section size first:
+    garbage, a foreign magic and a truncated image are ENC_ERR_INVALID_ARG
+    with no device involved."""
+    import ctypes as C
+    import numpy as np
+    lib = _lib.load()
+    out = C.c_void_p()
+    junk = np.zeros(128, np.uint8)
+    assert lib.enc_accel_deserialize(junk.ctypes.data, junk.size, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
+    assert b"not a serialised accelerator" in lib.enc_last_error()
+    short = np.frombuffer(b"ENCACC01", np.uint8).copy()
+    assert lib.enc_accel_deserialize(short.ctypes.data, short.size, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
+    # a well-formed header whose sections are missing
+    hdr = np.zeros(120, np.uint8)  # sizeof the header
+    hdr[:8] = np.frombuffer(b"ENCACC01", np.uint8)
+    hdr[8:12] = np.array([1], np.uint32).view(np.uint8)
+    assert lib.enc_accel_deserialize(hdr.ctypes.data, hdr.size, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
+    assert not out.value
