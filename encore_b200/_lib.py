@@ -187,6 +187,8 @@ SIGNATURES = {
                                                 C.POINTER(P)]),
     "enc_photonmap_create": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_destroy": (C.c_int32, [P]),
+    "enc_photonmap_serialize": (C.c_int32, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "enc_photonmap_deserialize": (C.c_int32, [P, C.c_size_t, C.c_int32, C.POINTER(P)]),
     "enc_photonmap_check": (C.c_int32, [P, P]),
     "enc_photonmap_radiance": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),
     "enc_photonmap_radiance_device": (C.c_int32, [P, P, P, C.c_size_t, C.c_int32, C.c_float, C.c_int32, P, P]),

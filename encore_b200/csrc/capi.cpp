@@ -999,6 +999,8 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
       d.lvl_off[l] = h.lvl_off[l];
       d.lvl_pad[l] = h.lvl_pad[l];
     }
+    d.box_floats = h.box.size();
+    d.leaf_words = h.leaf.size();
     e = upload(&d.d_box, h.box.data(), h.box.size());
     if (e == cudaSuccess) e = upload(&d.d_leaf, h.leaf.data(), h.leaf.size());
     if (e == cudaSuccess) e = upload(&d.d_pos4, h.pos4.data(), h.pos4.size());
@@ -1043,6 +1045,153 @@ enc_status enc_photonmap_create_device(const float* d_pos, const float* d_nrm, c
     }
   }
   return enc_photonmap_create(pos.data(), nrm.data(), pw.data(), n, caustic, device, out);
+}
+
+namespace {
+
+struct PhotonFileHeader {
+  char magic[8];
+  uint32_t version;
+  int32_t caustic;
+  uint32_t n, nnodes;
+  int32_t depth, nlevels;
+  uint32_t lvl_count[kPhotonMaxLevels], lvl_off[kPhotonMaxLevels], lvl_pad[kPhotonMaxLevels];
+  uint64_t box_floats, leaf_words;
+};
+constexpr char kPhotonMagic[8] = {'E', 'N', 'C', 'P', 'H', 'M', '0', '1'};
+
+}  // namespace
+
+enc_status enc_photonmap_serialize(enc_photonmap m, void* buf, size_t cap, size_t* size) {
+  if (!m || !size) {
+    set_error("enc_photonmap_serialize: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  const DevPhotonMap& d = m->dev;
+  PhotonFileHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kPhotonMagic, 8);
+  h.version = 1;
+  h.caustic = d.caustic;
+  h.n = d.n;
+  h.nnodes = d.nnodes;
+  h.depth = d.depth;
+  h.nlevels = d.nlevels;
+  for (int l = 0; l < kPhotonMaxLevels; ++l) {
+    h.lvl_count[l] = d.lvl_count[l];
+    h.lvl_off[l] = d.lvl_off[l];
+    h.lvl_pad[l] = d.lvl_pad[l];
+  }
+  h.box_floats = d.box_floats;
+  h.leaf_words = d.leaf_words;
+  const size_t body = 4 * h.box_floats + 4 * h.leaf_words + 3 * 16 * (size_t)h.n;
+  *size = sizeof(h) + body;
+  if (!buf) return ENC_OK;
+  if (cap < *size) {
+    set_error("enc_photonmap_serialize: buffer smaller than the size the call reports");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(m->mu);
+  DeviceScope ds(d.device);
+  char* p = static_cast<char*>(buf);
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  const void* src[5] = {d.d_box, d.d_leaf, d.d_pos4, d.d_nrm4, d.d_pow4};
+  const size_t bytes[5] = {4 * h.box_floats, 4 * h.leaf_words, 16 * (size_t)h.n,
+                           16 * (size_t)h.n, 16 * (size_t)h.n};
+  for (int i = 0; i < 5; ++i) {
+    if (bytes[i]) ENC_CUDA(cudaMemcpy(p, src[i], bytes[i], cudaMemcpyDeviceToHost), "read photon map");
+    p += bytes[i];
+  }
+  return ENC_OK;
+}
+
+enc_status enc_photonmap_deserialize(const void* buf, size_t size, int32_t device,
+                                     enc_photonmap* out) {
+  if (!buf || !out) {
+    set_error("enc_photonmap_deserialize: null argument");
+    return ENC_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  PhotonFileHeader h;
+  if (size < sizeof(h)) {
+    set_error("enc_photonmap_deserialize: shorter than the header");
+    return ENC_ERR_INVALID_ARG;
+  }
+  std::memcpy(&h, buf, sizeof(h));
+  auto bad = [](const char* why) {
+    set_error(std::string("enc_photonmap_deserialize: ") + why);
+    return ENC_ERR_INVALID_ARG;
+  };
+  if (std::memcmp(h.magic, kPhotonMagic, 8) != 0 || h.version != 1)
+    return bad("not a serialised photon map of this version");
+  if (h.nlevels < 0 || h.nlevels > kPhotonMaxLevels || h.n > 0x7fffffffu ||
+      (h.n > 0 && h.nlevels < 1))
+    return bad("level count or photon count out of range");
+  const size_t body = 4 * h.box_floats + 4 * h.leaf_words + 3 * 16 * (size_t)h.n;
+  if (size != sizeof(h) + body) return bad("sizes do not agree");
+  for (int l = 0; l < h.nlevels; ++l) {
+    if (h.lvl_count[l] > h.lvl_pad[l] || (uint64_t)h.lvl_off[l] + 6ull * h.lvl_pad[l] > h.box_floats)
+      return bad("a box level lies outside the box array");
+  }
+  if (h.nlevels > 0 && h.leaf_words != 2ull * h.lvl_count[0]) return bad("leaf table size");
+  // every leaf's photon range must lie inside the photon arrays, at most a
+  // warp's 32 photons: the gather reads photons by these ranges
+  const uint32_t* leaf = reinterpret_cast<const uint32_t*>(static_cast<const char*>(buf) +
+                                                           sizeof(h) + 4 * h.box_floats);
+  for (uint64_t i = 0; i < h.leaf_words / 2; ++i) {
+    uint32_t b, e;
+    std::memcpy(&b, leaf + 2 * i, 4);
+    std::memcpy(&e, leaf + 2 * i + 1, 4);
+    if (b > e || e > h.n || e - b > 32) return bad("a leaf's photon range is out of bounds");
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return bad("no such CUDA device");
+  DeviceScope ds(device);
+  enc_photonmap m = new (std::nothrow) enc_photonmap_s();
+  if (!m) return ENC_ERR_OUT_OF_MEMORY;
+  DevPhotonMap& d = m->dev;
+  d.caustic = h.caustic ? 1 : 0;
+  d.device = device;
+  d.n = h.n;
+  d.nnodes = h.nnodes;
+  d.depth = h.depth;
+  d.nlevels = h.nlevels;
+  for (int l = 0; l < kPhotonMaxLevels; ++l) {
+    d.lvl_count[l] = h.lvl_count[l];
+    d.lvl_off[l] = h.lvl_off[l];
+    d.lvl_pad[l] = h.lvl_pad[l];
+  }
+  d.box_floats = h.box_floats;
+  d.leaf_words = h.leaf_words;
+  const char* p = static_cast<const char*>(buf) + sizeof(h);
+  const float* fp = reinterpret_cast<const float*>(p);
+  cudaError_t e = upload(&d.d_box, fp, h.box_floats);
+  p += 4 * h.box_floats;
+  if (e == cudaSuccess) e = upload(&d.d_leaf, reinterpret_cast<const uint32_t*>(p), h.leaf_words);
+  p += 4 * h.leaf_words;
+  float** dst[3] = {&d.d_pos4, &d.d_nrm4, &d.d_pow4};
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+    e = upload(dst[i], reinterpret_cast<const float*>(p), 4 * (size_t)h.n);
+    p += 16 * (size_t)h.n;
+  }
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_status, 16);
+  if (e == cudaSuccess) e = cudaMemset(d.d_status, 0, 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d.d_counter, kGatherSlots * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    cudaFree(d.d_box);
+    cudaFree(d.d_leaf);
+    cudaFree(d.d_pos4);
+    cudaFree(d.d_nrm4);
+    cudaFree(d.d_pow4);
+    cudaFree(d.d_status);
+    cudaFree(d.d_counter);
+    delete m;
+    return cuda_fail(e, "enc_photonmap_deserialize");
+  }
+  *out = m;
+  return ENC_OK;
 }
 
 enc_status enc_photonmap_destroy(enc_photonmap m) {

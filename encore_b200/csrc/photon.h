@@ -74,6 +74,8 @@ struct DevPhotonMap {
   int depth = 0;
   int caustic = 0;
   int device = 0;
+  size_t box_floats = 0;   // PhotonHost::box.size()
+  size_t leaf_words = 0;   // PhotonHost::leaf.size()
 };
 
 // Launchers (gather.cu).  k <= 256.  Asynchronous on `stream`.

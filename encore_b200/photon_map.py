@@ -68,6 +68,32 @@ class PhotonMap:
         self.handle = h
         return self
 
+    def save(self) -> bytes:
+        """The balanced map as a byte image (enc_photonmap_serialize)."""
+        self.balance_and_construct()
+        size = C.c_size_t()
+        check(self.lib.enc_photonmap_serialize(self.handle, None, 0, C.byref(size)),
+              "enc_photonmap_serialize")
+        buf = np.empty(size.value, np.uint8)
+        check(self.lib.enc_photonmap_serialize(self.handle, ptr(buf), size.value, C.byref(size)),
+              "enc_photonmap_serialize")
+        return buf.tobytes()
+
+    @classmethod
+    def load(cls, image: bytes, device: int = 0) -> "PhotonMap":
+        """A map from a byte image saved by save(), with no host balance."""
+        buf = np.frombuffer(image, dtype=np.uint8)
+        lib = _lib.load()
+        h = C.c_void_p()
+        check(lib.enc_photonmap_deserialize(ptr(buf), buf.size, device, C.byref(h)),
+              "enc_photonmap_deserialize")
+        caustic = bool(int.from_bytes(image[12:16], "little"))
+        n = int.from_bytes(image[16:20], "little")
+        pm = cls(n, caustic=caustic, device=device)
+        pm.handle = h
+        pm._count = n
+        return pm
+
     def _flags(self, ignore_normal: bool) -> int:
         return _lib.ENC_GATHER_IGNORE_NORMAL if ignore_normal else 0
 

@@ -484,6 +484,13 @@ enc_status enc_photonmap_create(const float* pos, const float* normal, const flo
                                 size_t nphotons, int32_t caustic, int32_t device,
                                 enc_photonmap* out);
 enc_status enc_photonmap_destroy(enc_photonmap map);
+/* A balanced photon map saved as a byte image and loaded without the host
+ * balance (enc_accel_serialize's counterpart for photon maps; buf = NULL
+ * only sets *size).  Loading checks the header, the section sizes, the box
+ * levels and every leaf's photon range (ENC_ERR_INVALID_ARG on a mismatch). */
+enc_status enc_photonmap_serialize(enc_photonmap map, void* buf, size_t cap, size_t* size);
+enc_status enc_photonmap_deserialize(const void* buf, size_t size, int32_t device,
+                                     enc_photonmap* out);
 
 /* Gather flags. */
 enum {

@@ -65,3 +65,15 @@ def test_deserialize_rejects_malformed_images_before_any_device_call():
     hdr[8:12] = np.array([1], np.uint32).view(np.uint8)
     assert lib.enc_accel_deserialize(hdr.ctypes.data, hdr.size, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
     assert not out.value
+
+
+def test_photonmap_deserialize_rejects_malformed_images():
+    import ctypes as C
+    import numpy as np
+    lib = _lib.load()
+    out = C.c_void_p()
+    junk = np.zeros(256, np.uint8)
+    assert lib.enc_photonmap_deserialize(junk.ctypes.data, junk.size, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
+    assert b"not a serialised photon map" in lib.enc_last_error()
+    assert lib.enc_photonmap_deserialize(junk.ctypes.data, 8, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
+    assert not out.value

@@ -110,3 +110,28 @@ def test_nan_normals_never_match(gpu):
     q = pos[:10]
     assert np.all(pm.get_radiance_estimate(50, 1.0, q, nrm[:10]) == 0)
     assert np.all(pm.get_radiance_estimate(50, 1.0, q, nrm[:10], ignore_normal=True) > 0)
+
+
+def test_saved_and_loaded_photon_map_answers_identically(gpu):
+    """enc_photonmap_serialize / _deserialize: the loaded map (no host
+    balance) gives the same radiance and k-nearest sets bit for bit."""
+    rng = np.random.default_rng(97)
+    n = 30000
+    pos = rng.random((n, 3), dtype=np.float32) * 1000
+    nrm = np.tile(np.array([[0, 1, 0]], np.float32), (n, 1))
+    pw = rng.random((n, 3), dtype=np.float32)
+    q = rng.random((2000, 3), dtype=np.float32) * 1000
+    qn = np.tile(np.array([[0, 1, 0]], np.float32), (2000, 1))
+    for caustic in (False, True):
+        pm = PhotonMap(n, caustic=caustic)
+        pm.add_photons(pos, nrm, pw)
+        a = pm.get_radiance_estimate(50, 60.0, q, qn)
+        ia, da, ca = pm.get_nearest_n_photons(50, 60.0, q, qn)
+        img = pm.save()
+        pm2 = PhotonMap.load(img)
+        assert pm2.caustic == caustic and pm2.count() == n
+        b = pm2.get_radiance_estimate(50, 60.0, q, qn)
+        ib, db, cb = pm2.get_nearest_n_photons(50, 60.0, q, qn)
+        assert np.array_equal(a.view(np.int32), b.view(np.int32))
+        assert np.array_equal(ia, ib) and np.array_equal(ca, cb)
+        assert pm2.save() == img
