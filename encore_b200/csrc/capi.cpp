@@ -292,6 +292,7 @@ enc_status enc_accel_build(enc_scene scene, const enc_build_opts* opts, int32_t 
       make_dev_tris(scene->verts.data(), scene->ntris, nullptr, tris.data());
       d.nnodes = (uint32_t)h.nodes.size();
       d.kd_nitems = (uint32_t)h.items.size();
+      d.tree_depth = h.max_depth + 1;  // levels below the root: one deferred child each
       for (int i = 0; i < 3; ++i) {
         d.kd_root_lo[i] = h.root_lo[i];
         d.kd_root_hi[i] = h.root_hi[i];
@@ -390,6 +391,7 @@ enc_status enc_accel_refit(enc_accel a, const float* tri_verts, uint32_t ntris) 
       d.d_kd_items = items;
       d.nnodes = (uint32_t)h.nodes.size();
       d.kd_nitems = (uint32_t)h.items.size();
+      d.tree_depth = h.max_depth + 1;
       d.node_bytes = h.nodes.size() * sizeof(KdNode) + h.items.size() * sizeof(uint32_t);
       for (int i = 0; i < 3; ++i) {
         d.kd_root_lo[i] = h.root_lo[i];

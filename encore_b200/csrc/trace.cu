@@ -766,9 +766,11 @@ struct KdParams {
   float lo[3], hi[3];  // root box min corner and pos + size
 };
 
-constexpr int kKdStack = 64;
-
-template <bool CLAMP, bool ANY>
+// Deferred far children of the walk: at most one per level, so a tree of
+// depth <= 32 (the reference's depth limit 11 + 1.3 ln N stays below 32 up
+// to about 10M triangles) needs 32 entries; deeper trees get 64.  The
+// stack lives in local memory: the smaller one halves its traffic.
+template <bool CLAMP, bool ANY, int kKdStack>
 __global__ void __launch_bounds__(128) kd_trace(KdParams P) {
   for (unsigned qi = blockIdx.x * blockDim.x + threadIdx.x; qi < P.nrays;
        qi += gridDim.x * blockDim.x) {
@@ -824,12 +826,16 @@ __global__ void __launch_bounds__(128) kd_trace(KdParams P) {
           const int axis = (int)(n.word0 & 3u);
           float split = __uint_as_float(n.word0);
           split = (split > -0.001f && split < 0.001f) ? 0.0f : split;
-          const float tplane = fm(fs(split, o[axis]), inv[axis]);
-          const bool below = o[axis] <= split;
+          // the axis's origin and reciprocal by select, not by indexing the
+          // arrays with the runtime axis (which would put them in local memory)
+          const float oa = axis == 0 ? o[0] : (axis == 1 ? o[1] : o[2]);
+          const float ia = axis == 0 ? inv[0] : (axis == 1 ? inv[1] : inv[2]);
+          const float tplane = fm(fs(split, oa), ia);
+          const bool below = oa <= split;
           const uint32_t first = below ? n.word1 : n.word1 + 1;
           const uint32_t second = below ? n.word1 + 1 : n.word1;
           if (tplane == 0.0f) {
-            node = inv[axis] > 0.0f ? second : first;
+            node = ia > 0.0f ? second : first;
           } else if (tplane >= tmax || tplane < 0.0f) {
             node = first;
           } else if (tplane <= tmin) {
@@ -981,10 +987,14 @@ int launch_kd(const DevAccel& a, const float* rays, size_t n, void* out, cudaStr
   unsigned need = (unsigned)((n + 127) / 128);
   if ((unsigned)grid > need) grid = (int)need;
   if (grid < 1) grid = 1;
-  if (a.predicate == ENC_PRED_REFERENCE)
-    kd_trace<true, ANY><<<grid, 128, 0, s>>>(p);
-  else
-    kd_trace<false, ANY><<<grid, 128, 0, s>>>(p);
+  const bool small = a.tree_depth > 0 && a.tree_depth <= 32;
+  if (a.predicate == ENC_PRED_REFERENCE) {
+    if (small) kd_trace<true, ANY, 32><<<grid, 128, 0, s>>>(p);
+    else kd_trace<true, ANY, 64><<<grid, 128, 0, s>>>(p);
+  } else {
+    if (small) kd_trace<false, ANY, 32><<<grid, 128, 0, s>>>(p);
+    else kd_trace<false, ANY, 64><<<grid, 128, 0, s>>>(p);
+  }
   return (int)cudaGetLastError();
 }
 
