@@ -68,7 +68,10 @@ constexpr int kBins = 16;
 // leaves of up to 3 triangles the trees barely change; with up to 4 the
 // extra triangle tests cost 14-24 % more time than the fewer node visits
 // save.)
-constexpr float kTravCost = 1.0f;
+#ifndef ENC_SAH_TRAV_COST
+#define ENC_SAH_TRAV_COST 1.0f
+#endif
+constexpr float kTravCost = ENC_SAH_TRAV_COST;
 constexpr uint32_t kParallelCutoff = 1u << 16;
 
 struct BinaryBuilder {
