@@ -34,13 +34,14 @@
 
 // Resident 128-thread blocks per SM that each kernel's register budget is
 // fitted to (also the default grid: SMs x this).  The closest-hit kernel
-// tests triangles cooperatively across the warp (below), which needs 64
-// registers: at 8 blocks it ran 4.5 % faster than the per-lane loop at its
-// best (10 blocks, 48 registers) on the 2M-triangle heightfield workload,
-// while at 9 or 10 blocks its spills cost more than the extra warps gave.
-// The any-hit kernel keeps the per-lane loop (its rays rarely reach a
-// triangle before the first hit) and 10 blocks.
-constexpr int kBlocksClosest = 8;
+// tests triangles cooperatively across the warp (below).  At 9 blocks it fits
+// 56 registers without spilling and ran 1.7 % faster than at 8 (64
+// registers) on the 2M-triangle heightfield workload; at 10 blocks (48
+// registers) it spills 42 bytes and lost 8 %.  The multi-scene form keeps 8
+// blocks: at 9 it spills 78 bytes.  The any-hit kernel keeps the per-lane
+// loop (its rays rarely reach a triangle before the first hit) and 10 blocks.
+constexpr int kBlocksClosest = 9;
+constexpr int kBlocksMulti = 8;
 constexpr int kBlocksAny = 10;
 
 namespace enc {
@@ -229,7 +230,8 @@ __device__ __forceinline__ void sort_net<4>(float (&k)[4], uint32_t (&v)[4]) {
 #undef ENC_CSWAP
 
 template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false, bool LANE = false>
-__global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny : kBlocksClosest)
+__global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
+                                                     : (MULTI ? kBlocksMulti : kBlocksClosest))
     wbvh_trace(TraceParams P) {
   using L = WNodeLayout<W>;
   // Stack of node groups: one entry per visited node that still has hit
@@ -1215,7 +1217,7 @@ int launch_multi_w(const MultiLaunch& m, const Launch& L, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(m.d_counter, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return (int)e;
   int grid = device_sm_count(m.device) *
-             (L.blocks_per_sm > 0 ? L.blocks_per_sm : (ANY ? kBlocksAny : kBlocksClosest));
+             (L.blocks_per_sm > 0 ? L.blocks_per_sm : (ANY ? kBlocksAny : kBlocksMulti));
   k<<<grid, L.block, smem, s>>>(p);
   return (int)cudaGetLastError();
 }
