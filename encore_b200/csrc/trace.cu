@@ -168,6 +168,17 @@ constexpr uint32_t kNoItem = 0xffffffffu;
 #ifndef ENC_F32X2
 #define ENC_F32X2 1
 #endif
+#ifndef ENC_GROUP_BOUND
+#define ENC_GROUP_BOUND 0
+#endif
+// Width 8, closest hit: the stack group's lower bound (the smallest entry
+// distance among the node's hit internal children) includes the child the
+// walk continues into, and the hit found under that child is rarely nearer
+// than its entry, so a popped group was culled by it 0.0002 times per ray on
+// the 2M-triangle heightfield batch.  Without it such a group's node is
+// visited and every child fails the box test against the same closest hit
+// (so the hits are identical) and the per-child bound work is saved.
+constexpr bool kGroupBound = ENC_GROUP_BOUND != 0;
 constexpr bool kPairs = ENC_F32X2 != 0;
 
 __device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
@@ -253,6 +264,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
   // Closest hit tests the triangles of the lanes' hit leaves as one warp
   // (see below); any hit, and closest hit with LANE, keep one loop per lane.
   constexpr bool kCoop = !ANY && !LANE;
+  // the per-lane form keeps the group bound (without it ptxas spills more)
+  constexpr bool kBound = kGroupBound || LANE;
   __shared__ uint32_t s_coop_tri[kCoop ? 128 : 1];
   __shared__ uint32_t s_coop_own[kCoop ? 128 : 1];
   __shared__ unsigned long long s_coop_key[kCoop ? 128 : 1];
@@ -532,7 +545,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
             if (tn <= tf) {
               hm |= 1u << c;
               // (any hit never culls by distance, so it keeps no bound)
-              if (!ANY && ((imask >> c) & 1u)) lbmin = fminf(lbmin, tn);
+              if (!ANY && kBound && ((imask >> c) & 1u)) lbmin = fminf(lbmin, tn);
             }
           }
           // triangles of the hit leaves (meta = count << 5 | offset)
@@ -596,7 +609,8 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
               } else {
                 if constexpr (kCompact) {
                   const uint32_t lb16 =
-                      ANY ? 0u : (lbmin >= 0.0f ? (__float_as_uint(lbmin) >> 16) : 0xff80u);
+                      (ANY || !kBound) ? 0u
+                                            : (lbmin >= 0.0f ? (__float_as_uint(lbmin) >> 16) : 0xff80u);
                   stk[sp * B] = make_uint2(child_base, rest | (imask << 8) | (lb16 << 16));
                 } else {
                   stk[sp * B] = make_uint2(child_base, rest | (imask << 8));
@@ -774,7 +788,7 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
           uint2 e;
           if constexpr (kCompact) {
             e = stk[(sp - 1) * B];
-            if (!ANY && __uint_as_float(e.y & 0xffff0000u) > best_t) {
+            if (!ANY && kBound && __uint_as_float(e.y & 0xffff0000u) > best_t) {
               --sp;
               continue;
             }
