@@ -539,9 +539,16 @@ __global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
               tnz = fmaf(__uint_as_float(__byte_perm(wn[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
               tfz = fmaf(__uint_as_float(__byte_perm(wf[4 + h], 0x4B000000u, sel)) - 8388608.0f, cz, bz);
             }
-            // (three-input min/max measured 1.6 % slower here)
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, vtmin));
-            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+            // sm_100's three-input max/min (NaN operands ignored, as fmaxf /
+            // fminf do): +0.45 % over the two-input tree
+            float tn, tf;
+            {
+              float m;
+              asm("max.f32 %0, %1, %2, %3;" : "=f"(m) : "f"(tnx), "f"(tny), "f"(tnz));
+              tn = fmaxf(m, vtmin);
+              asm("min.f32 %0, %1, %2, %3;" : "=f"(m) : "f"(tfx), "f"(tfy), "f"(tfz));
+              tf = fminf(m, best_t);
+            }
             if (tn <= tf) {
               hm |= 1u << c;
               // (any hit never culls by distance, so it keeps no bound)
