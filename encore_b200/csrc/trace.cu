@@ -39,10 +39,14 @@
 // registers) on the 2M-triangle heightfield workload; at 10 blocks (48
 // registers) it spills 42 bytes and lost 8 %.  The multi-scene form keeps 8
 // blocks: at 9 it spills 78 bytes.  The any-hit kernel keeps the per-lane
-// loop (its rays rarely reach a triangle before the first hit) and 10 blocks.
+// loop (its rays rarely reach a triangle before the first hit) at 9 blocks
+// (no spill; 3.9 % faster than 10 with a 28-byte spill).  The per-lane
+// closest-hit form, which the host-buffer pipeline runs beside its copies,
+// keeps 10 (at 9 the pipeline measured about 1 % slower).
 constexpr int kBlocksClosest = 9;
 constexpr int kBlocksMulti = 8;
-constexpr int kBlocksAny = 10;
+constexpr int kBlocksAny = 9;
+constexpr int kBlocksLane = 10;
 
 namespace enc {
 namespace {
@@ -241,8 +245,9 @@ __device__ __forceinline__ void sort_net<4>(float (&k)[4], uint32_t (&v)[4]) {
 #undef ENC_CSWAP
 
 template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false, bool LANE = false>
-__global__ void __launch_bounds__(128, (ANY || LANE) ? kBlocksAny
-                                                     : (MULTI ? kBlocksMulti : kBlocksClosest))
+__global__ void __launch_bounds__(128, ANY    ? kBlocksAny
+                                      : LANE ? kBlocksLane
+                                             : (MULTI ? kBlocksMulti : kBlocksClosest))
     wbvh_trace(TraceParams P) {
   using L = WNodeLayout<W>;
   // Stack of node groups: one entry per visited node that still has hit
@@ -1047,7 +1052,8 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
   cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return (int)e;
   int grid = device_sm_count(a.device) *
-             (L.blocks_per_sm > 0 ? L.blocks_per_sm : ((ANY || lane) ? kBlocksAny : kBlocksClosest));
+             (L.blocks_per_sm > 0 ? L.blocks_per_sm
+                                  : (ANY ? kBlocksAny : (lane ? kBlocksLane : kBlocksClosest)));
   k<<<grid, L.block, smem, s>>>(p);
   return (int)cudaGetLastError();
 }
