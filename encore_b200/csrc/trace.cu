@@ -215,6 +215,40 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
   return r;
 }
 
+
+// L2 eviction priorities: rays are read once and hits written once, so they
+// go in as evict_first, and the nodes, read by every ray, as evict_last; the
+// streaming data then displaces less of the node and triangle working set
+// (about the L2's size on the 2M-triangle heightfield).  +0.36 %, identical
+// hits.
+__device__ __forceinline__ uint64_t l2_policy_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float4 ldg_hint(const float4* a, uint64_t pol) {
+  float4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint4 ldg_hint_u(const uint4* a, uint64_t pol) {
+  uint4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void stg_hint(int4* a, int4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.s32 [%0], {%1,%2,%3,%4}, %5;" ::"l"(a), "r"(v.x),
+               "r"(v.y), "r"(v.z), "r"(v.w), "l"(pol)
+               : "memory");
+}
+
 template <int W>
 __device__ __forceinline__ void sort_net(float (&k)[W], uint32_t (&v)[W]);
 
@@ -395,8 +429,8 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           l_idx = (unsigned)ray;
           rp = P.rays + 2 * (size_t)ray;
         }
-        const float4 r0 = __ldg(rp);
-        const float4 r1 = __ldg(rp + 1);
+        const float4 r0 = ldg_hint(rp, l2_policy_first());
+        const float4 r1 = ldg_hint(rp + 1, l2_policy_first());
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
 
@@ -456,7 +490,7 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
         NodeWords<W> nw;
         const uint4* src = reinterpret_cast<const uint4*>(l_nodes + (size_t)node * L::kBytes);
 #pragma unroll
-        for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = __ldg(src + i);
+        for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = ldg_hint_u(src + i, l2_policy_last());
         const float px = __uint_as_float(nw.w[0].x);
         const float py = __uint_as_float(nw.w[0].y);
         const float pz = __uint_as_float(nw.w[0].z);
@@ -848,7 +882,7 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           h.y = best_id >= 0 ? __float_as_int(best_t) : 0;
           h.z = best_id >= 0 ? __float_as_int(bu) : 0;
           h.w = best_id >= 0 ? __float_as_int(bv) : 0;
-          reinterpret_cast<int4*>(l_out)[l_idx] = h;
+          stg_hint(reinterpret_cast<int4*>(l_out) + l_idx, h, l2_policy_first());
         }
         if (COUNT) {
           P.visits[2 * (size_t)ray] = nvis;
