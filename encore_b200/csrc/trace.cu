@@ -219,8 +219,8 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
 // L2 eviction priorities: rays are read once and hits written once, so they
 // go in as evict_first, and the nodes, read by every ray, as evict_last; the
 // streaming data then displaces less of the node and triangle working set
-// (about the L2's size on the 2M-triangle heightfield).  +0.36 %, identical
-// hits.
+// (about the L2's size on the 2M-triangle heightfield).  +0.36 % for the
+// cooperative closest-hit kernel, identical hits.
 __device__ __forceinline__ uint64_t l2_policy_first() {
   uint64_t p;
   asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
@@ -305,6 +305,12 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
   constexpr bool kCoop = !ANY && !LANE;
   // the per-lane form keeps the group bound (without it ptxas spills more)
   constexpr bool kBound = kGroupBound || LANE;
+  // L2 priorities in the single-scene cooperative closest-hit form only: in
+  // any hit they measured 1 % slower, and in the per-lane form, which the
+  // host-buffer pipeline runs, the evict_first hits left L2 before their copy
+  // out (2 %); the multi-scene form, whose hits the server copies out after
+  // each launch, keeps plain loads and stores too
+  constexpr bool kL2Hints = kCoop && !MULTI;
   __shared__ uint32_t s_coop_tri[kCoop ? 128 : 1];
   __shared__ uint32_t s_coop_own[kCoop ? 128 : 1];
   __shared__ unsigned long long s_coop_key[kCoop ? 128 : 1];
@@ -429,8 +435,8 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           l_idx = (unsigned)ray;
           rp = P.rays + 2 * (size_t)ray;
         }
-        const float4 r0 = ldg_hint(rp, l2_policy_first());
-        const float4 r1 = ldg_hint(rp + 1, l2_policy_first());
+        const float4 r0 = kL2Hints ? ldg_hint(rp, l2_policy_first()) : __ldg(rp);
+        const float4 r1 = kL2Hints ? ldg_hint(rp + 1, l2_policy_first()) : __ldg(rp + 1);
         ox = r0.x; oy = r0.y; oz = r0.z; tmin = r0.w;
         dx = r1.x; dy = r1.y; dz = r1.z; tmax = r1.w;
 
@@ -490,7 +496,8 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
         NodeWords<W> nw;
         const uint4* src = reinterpret_cast<const uint4*>(l_nodes + (size_t)node * L::kBytes);
 #pragma unroll
-        for (int i = 0; i < NodeWords<W>::N; ++i) nw.w[i] = ldg_hint_u(src + i, l2_policy_last());
+        for (int i = 0; i < NodeWords<W>::N; ++i)
+          nw.w[i] = kL2Hints ? ldg_hint_u(src + i, l2_policy_last()) : __ldg(src + i);
         const float px = __uint_as_float(nw.w[0].x);
         const float py = __uint_as_float(nw.w[0].y);
         const float pz = __uint_as_float(nw.w[0].z);
@@ -882,7 +889,10 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           h.y = best_id >= 0 ? __float_as_int(best_t) : 0;
           h.z = best_id >= 0 ? __float_as_int(bu) : 0;
           h.w = best_id >= 0 ? __float_as_int(bv) : 0;
-          stg_hint(reinterpret_cast<int4*>(l_out) + l_idx, h, l2_policy_first());
+          if (kL2Hints)
+            stg_hint(reinterpret_cast<int4*>(l_out) + l_idx, h, l2_policy_first());
+          else
+            reinterpret_cast<int4*>(l_out)[l_idx] = h;
         }
         if (COUNT) {
           P.visits[2 * (size_t)ray] = nvis;
