@@ -278,7 +278,8 @@ __device__ __forceinline__ void sort_net<4>(float (&k)[4], uint32_t (&v)[4]) {
 }
 #undef ENC_CSWAP
 
-template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false, bool LANE = false>
+template <int W, bool CLAMP, bool ANY, bool COUNT, bool MULTI = false, bool LANE = false,
+          bool ORD = false>
 __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
                                       : LANE ? kBlocksLane
                                              : (MULTI ? kBlocksMulti : kBlocksClosest))
@@ -335,7 +336,9 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
   // loaded once when the chunk is taken (one coalesced load per chunk instead
   // of a dependent load per refill); chunks above 32 rays read the rest
   // directly.
-  constexpr bool kOrdered = !MULTI && !ANY;  // binned batches: closest hit only
+  // binned batches (closest hit only): a separate instantiation, so the plain
+  // launch carries none of the order handling
+  constexpr bool kOrdered = ORD && !MULTI && !ANY;
   unsigned pool_base = 0, ord_reg = 0;
 
   int ray = -1;
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           // prefetch; the warp that claims it later finds it in L2).  With the
           // round's atomic listing below: +1.7 % on the 2M-triangle
           // heightfield batch (the listing alone measured -1.2 %).
-          if (!MULTI && P.order == nullptr) {
+          if (!MULTI && !kOrdered) {
             const unsigned ahead = gridDim.x * (blockDim.x >> 5) * (unsigned)P.chunk;
             const unsigned pb = b + ahead;
             if (pb > b && pb < P.nrays) {
@@ -1088,7 +1091,15 @@ int launch_w(const DevAccel& a, const float* rays, size_t n, void* out, uint32_t
   p.chunk = L.chunk;
   size_t smem = (size_t)p.stack_depth * L.block * stack_entry_bytes(W);
   const bool lane = !ANY && L.per_lane;
-  auto k = lane ? wbvh_trace<W, CLAMP, ANY, COUNT, false, true> : wbvh_trace<W, CLAMP, ANY, COUNT>;
+  // Binned (ordered) launches use their own instantiation (closest hit
+  // only); without the order handling the plain cooperative kernel ran 1.6 %
+  // faster.  The per-lane form, which the host-buffer pipeline runs beside
+  // its copies, keeps it whatever the order: leaner, it ran faster but slowed
+  // the concurrent copies more (the whole call 4 % slower).
+  const bool ord = !ANY && order != nullptr;
+  auto k = lane ? wbvh_trace<W, CLAMP, ANY, COUNT, false, true, true>
+                : (ord ? wbvh_trace<W, CLAMP, ANY, COUNT, false, false, true>
+                       : wbvh_trace<W, CLAMP, ANY, COUNT>);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
