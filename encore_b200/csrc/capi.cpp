@@ -902,12 +902,6 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     a->ev_in.push_back(e1);
     a->ev_trace.push_back(e2);
   }
-  // The chunks' traces run beside the copies, and the copy in is the
-  // bottleneck: the per-lane closest-hit kernel (10 blocks per SM) slows the
-  // copies less than the faster warp-cooperative one, and the whole call ran
-  // 8-9 % faster with it (1,371 against 1,260 Mrays/s on the 4.18M-ray
-  // bench batch, the same box, back to back).
-  L.per_lane = true;
   cudaStream_t cin = a->pipe[0], ctr = a->pipe[1], cout = a->pipe[2];
   ENC_CUDA(cudaEventRecord(a->pipe_start, s), "event record");
   for (int i = 0; i < 3; ++i) ENC_CUDA(cudaStreamWaitEvent(a->pipe[i], a->pipe_start, 0), "wait");
@@ -920,8 +914,12 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
   for (size_t c = 0; c < nch; ++c) {
     const size_t b = bound[c], n = bound[c + 1] - b;
     ENC_CUDA(cudaStreamWaitEvent(ctr, a->ev_in[c], 0), "wait");
-    // the last chunk has no copy in beside it: the faster warp-cooperative
-    // kernel shortens the call's tail (+1.4 % on the 4.18M-ray batch)
+    // The chunks' traces run beside the copies, and the copy in is the
+    // bottleneck: the per-lane closest-hit kernel (10 blocks per SM) slows
+    // the copies less than the faster warp-cooperative one (the whole call ran
+    // 8-9 % faster with it on the 4.18M-ray bench batch, and 4-7 % faster
+    // against today's cooperative kernel).  The last chunk has no copy in
+    // beside it: the cooperative kernel shortens the call's tail (+1.4 %).
     L.per_lane = c + 1 < nch;
     int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr)
                 : launch_closest(a->dev, (const float*)(din + b * 32), n,
