@@ -917,9 +917,9 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     // The chunks' traces run beside the copies, and the copy in is the
     // bottleneck: the per-lane closest-hit kernel (10 blocks per SM) slows
     // the copies less than the faster warp-cooperative one (the whole call ran
-    // 8-9 % faster with it on the 4.18M-ray bench batch, and 4-7 % faster
-    // against today's cooperative kernel).  The last chunk has no copy in
-    // beside it: the cooperative kernel shortens the call's tail (+1.4 %).
+    // 4-9 % faster with it on the 4.18M-ray bench batch).  The last chunk has
+    // no copy in beside it: the cooperative kernel shortens the call's tail
+    // (+1.4 %).
     L.per_lane = c + 1 < nch;
     int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr)
                 : launch_closest(a->dev, (const float*)(din + b * 32), n,
