@@ -829,8 +829,6 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
         } else if (nk != mykey) {
           best_t = from_order_key((uint32_t)(nk >> 32));
           best_id = (int)(uint32_t)nk;
-          bu = uv[lane].x;
-          bv = uv[lane].y;
         }
         __syncwarp();
         pend = __ballot_sync(kFull, tmask != 0);
@@ -890,8 +888,15 @@ __global__ void __launch_bounds__(128, ANY    ? kBlocksAny
           int4 h;
           h.x = best_id;
           h.y = best_id >= 0 ? __float_as_int(best_t) : 0;
-          h.z = best_id >= 0 ? __float_as_int(bu) : 0;
-          h.w = best_id >= 0 ? __float_as_int(bv) : 0;
+          float hu = bu, hv = bv;
+          if constexpr (kCoop) {
+            // the round that found the hit left its barycentrics in shared memory
+            const float2 w = s_coop_uv[threadIdx.x];
+            hu = w.x;
+            hv = w.y;
+          }
+          h.z = best_id >= 0 ? __float_as_int(hu) : 0;
+          h.w = best_id >= 0 ? __float_as_int(hv) : 0;
           if (kL2Hints)
             stg_hint(reinterpret_cast<int4*>(l_out) + l_idx, h, l2_policy_first());
           else
