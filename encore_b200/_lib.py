@@ -142,6 +142,7 @@ SIGNATURES = {
     "enc_accel_deserialize": (C.c_int32, [P, C.c_size_t, C.c_int32, C.POINTER(P)]),
     "enc_accel_info_get": (C.c_int32, [P, C.POINTER(AccelInfo)]),
     "enc_intersect_closest": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
+    "enc_intersect_closest_od": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_intersect_closest_device": (C.c_int32, [P, P, C.c_size_t, P, C.POINTER(LaunchOpts), P]),
     "enc_bin_scratch_bytes": (C.c_int32, [C.c_size_t, C.POINTER(BinOpts),
                                           C.POINTER(C.c_size_t)]),

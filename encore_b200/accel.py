@@ -162,6 +162,23 @@ class Accelerator:
                                              _stream_ptr(stream)), "enc_intersect_closest")
         return hits
 
+    # AccelerationStructure::intersect on the reference's Ray payload: (N, 6)
+    # float32 origin and direction, no distance bounds (a hit needs t > 0)
+    def intersect_od(self, rays, launch: LaunchConfig | None = None, stream=None,
+                     out: np.ndarray | None = None) -> np.ndarray:
+        if isinstance(rays, np.ndarray):
+            r = np.ascontiguousarray(rays, dtype=np.float32)
+            if r.ndim != 2 or r.shape[1] != 6:
+                raise ValueError("rays must be (N, 6) float32: ox oy oz dx dy dz")
+        else:
+            r = rays
+        n = r.shape[0]
+        hits = out if out is not None else np.empty(n, dtype=HIT_DTYPE)
+        lo = (launch or LaunchConfig()).c()
+        check(self.lib.enc_intersect_closest_od(self.handle, ptr(r), n, ptr(hits), C.byref(lo),
+                                                _stream_ptr(stream)), "enc_intersect_closest_od")
+        return hits
+
     def occluded(self, rays: np.ndarray, launch: LaunchConfig | None = None, stream=None,
                  out: np.ndarray | None = None) -> np.ndarray:
         r = _as_rays(rays) if isinstance(rays, np.ndarray) else rays

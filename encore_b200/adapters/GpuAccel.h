@@ -98,6 +98,11 @@ class GpuAccel : public AccelerationStructure {
   enc_status intersectBatch(const float* rays8, size_t n, enc_hit* hits) {
     return enc_intersect_closest(m_accel, rays8, n, hits, NULL, NULL);
   }
+  // n rays of 6 floats (ox oy oz dx dy dz: a Ray's origin and direction, no
+  // distance bounds) -> n hits; 24 bytes per ray cross PCIe instead of 32.
+  enc_status intersectBatchOD(const float* rays6, size_t n, enc_hit* hits) {
+    return enc_intersect_closest_od(m_accel, rays6, n, hits, NULL, NULL);
+  }
   enc_status occludedBatch(const float* rays8, size_t n, uint8_t* occluded) {
     return enc_intersect_any(m_accel, rays8, n, occluded, NULL, NULL);
   }

@@ -23,7 +23,8 @@ struct enc_accel_s {
   std::mutex mu;  // serialises the host-buffer forms (shared staging buffers)
   void* d_stage_in = nullptr;
   void* d_stage_out = nullptr;
-  size_t stage_in_bytes = 0, stage_out_bytes = 0;
+  void* d_stage_od = nullptr;  // rays of 6 floats, before widening (enc_intersect_closest_od)
+  size_t stage_in_bytes = 0, stage_out_bytes = 0, stage_od_bytes = 0;
   // host-form pipeline: copy-in, trace and copy-out streams, and per-chunk
   // events (copy-in done, trace done)
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
@@ -620,6 +621,7 @@ enc_status enc_accel_destroy(enc_accel a) {
   free_dev(a->dev);
   free_wave_scratch(&a->wave);
   cudaFree(a->d_stage_in);
+  cudaFree(a->d_stage_od);
   cudaFree(a->d_stage_out);
   for (int i = 0; i < 3; ++i)
     if (a->pipe[i]) cudaStreamDestroy(a->pipe[i]);
@@ -838,9 +840,12 @@ namespace {
 // 1M and 2M; the earlier two-stream form, whose copy in of chunk i+2 queued
 // behind chunk i's copy out, was 15 % slower.)  Ordering with the caller's
 // stream is kept with events; the call returns after the results are in
-// `out`.
+// `out`.  ray_floats = 8: rays in the traversal's layout; 6 (closest hit
+// only): origin and direction, copied in at 24 bytes per ray and widened on
+// the trace stream ahead of each chunk's trace.
 enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, size_t out_bytes,
-                     bool any, const enc_launch_opts* launch, enc_stream stream, const char* what) {
+                     bool any, int ray_floats, const enc_launch_opts* launch, enc_stream stream,
+                     const char* what) {
   if (!a || (nrays && (!rays || !out))) {
     set_error(std::string(what) + ": null argument");
     return ENC_ERR_INVALID_ARG;
@@ -859,16 +864,28 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
   std::lock_guard<std::mutex> lk(a->mu);
   DeviceScope ds(a->dev.device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool od = ray_floats == 6;
+  const size_t rb = (size_t)ray_floats * sizeof(float);  // bytes per ray in `rays`
   enc_status st = grow(&a->d_stage_in, &a->stage_in_bytes, nrays * 32);
   if (st) return st;
   st = grow(&a->d_stage_out, &a->stage_out_bytes, nrays * out_bytes);
   if (st) return st;
+  if (od) {
+    st = grow(&a->d_stage_od, &a->stage_od_bytes, nrays * rb);
+    if (st) return st;
+  }
   const size_t kChunk = (size_t)1 << 19;
   const size_t nchunks = nrays <= 2 * kChunk ? 1 : (nrays + kChunk - 1) / kChunk;
-  const char* din = static_cast<const char*>(a->d_stage_in);
+  char* din = static_cast<char*>(a->d_stage_in);
   char* dout = static_cast<char*>(a->d_stage_out);
+  // where a chunk's rays land: the traversal layout, or the 6-float staging
+  char* dcopy = od ? static_cast<char*>(a->d_stage_od) : din;
   if (nchunks == 1) {
-    ENC_CUDA(cudaMemcpyAsync(a->d_stage_in, rays, nrays * 32, cudaMemcpyHostToDevice, s), "H2D rays");
+    ENC_CUDA(cudaMemcpyAsync(dcopy, rays, nrays * rb, cudaMemcpyHostToDevice, s), "H2D rays");
+    if (od) {
+      const int e = launch_widen_rays((const float*)dcopy, nrays, (float*)din, a->dev.device, s);
+      if (e) return cuda_fail((cudaError_t)e, "ray widen launch");
+    }
     int e = any ? launch_any(a->dev, (const float*)din, nrays, (uint8_t*)dout, L, s)
                 : launch_closest(a->dev, (const float*)din, nrays, (enc_hit*)dout, L, s, nullptr);
     if (e) return cuda_fail((cudaError_t)e, "trace launch");
@@ -907,20 +924,29 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
   for (int i = 0; i < 3; ++i) ENC_CUDA(cudaStreamWaitEvent(a->pipe[i], a->pipe_start, 0), "wait");
   for (size_t c = 0; c < nch; ++c) {
     const size_t b = bound[c], n = bound[c + 1] - b;
-    ENC_CUDA(cudaMemcpyAsync((void*)(din + b * 32), rays + 8 * b, n * 32, cudaMemcpyHostToDevice, cin),
+    ENC_CUDA(cudaMemcpyAsync(dcopy + b * rb, rays + (size_t)ray_floats * b, n * rb,
+                             cudaMemcpyHostToDevice, cin),
              "H2D rays");
     ENC_CUDA(cudaEventRecord(a->ev_in[c], cin), "event record");
   }
   for (size_t c = 0; c < nch; ++c) {
     const size_t b = bound[c], n = bound[c + 1] - b;
     ENC_CUDA(cudaStreamWaitEvent(ctr, a->ev_in[c], 0), "wait");
-    // The chunks' traces run beside the copies, and the copy in is the
-    // bottleneck: the per-lane closest-hit kernel (10 blocks per SM) slows
-    // the copies less than the faster warp-cooperative one (the whole call ran
-    // 4-9 % faster with it on the 4.18M-ray bench batch).  The last chunk has
-    // no copy in beside it: the cooperative kernel shortens the call's tail
-    // (+1.4 %).
-    L.per_lane = c + 1 < nch;
+    // The chunks' traces run beside the copies.  With 32-byte rays the copy
+    // in is the bottleneck: the per-lane closest-hit kernel (10 blocks per
+    // SM) slows the copies less than the faster warp-cooperative one (the
+    // whole call ran 4-9 % faster with it on the 4.18M-ray bench batch), and
+    // only the last chunk, which has no copy in beside it, runs the
+    // cooperative kernel to shorten the call's tail (+1.4 %).  With 24-byte
+    // rays a chunk's copy in is shorter than its per-lane trace, so every
+    // chunk runs the cooperative kernel (1,693 against 1,428 Mrays/s on the
+    // bench batch, four rounds each).
+    L.per_lane = !od && c + 1 < nch;
+    if (od) {
+      const int e = launch_widen_rays((const float*)(dcopy + b * rb), n, (float*)(din + b * 32),
+                                      a->dev.device, ctr);
+      if (e) return cuda_fail((cudaError_t)e, "ray widen launch");
+    }
     int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr)
                 : launch_closest(a->dev, (const float*)(din + b * 32), n,
                                  (enc_hit*)(dout + b * sizeof(enc_hit)), L, ctr, nullptr);
@@ -940,13 +966,19 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
 
 enc_status enc_intersect_closest(enc_accel a, const float* rays, size_t nrays, enc_hit* hits,
                                  const enc_launch_opts* launch, enc_stream stream) {
-  return host_form(a, rays, nrays, hits, sizeof(enc_hit), false, launch, stream,
+  return host_form(a, rays, nrays, hits, sizeof(enc_hit), false, 8, launch, stream,
                    "enc_intersect_closest");
+}
+
+enc_status enc_intersect_closest_od(enc_accel a, const float* rays, size_t nrays, enc_hit* hits,
+                                    const enc_launch_opts* launch, enc_stream stream) {
+  return host_form(a, rays, nrays, hits, sizeof(enc_hit), false, 6, launch, stream,
+                   "enc_intersect_closest_od");
 }
 
 enc_status enc_intersect_any(enc_accel a, const float* rays, size_t nrays, uint8_t* occ,
                              const enc_launch_opts* launch, enc_stream stream) {
-  return host_form(a, rays, nrays, occ, 1, true, launch, stream, "enc_intersect_any");
+  return host_form(a, rays, nrays, occ, 1, true, 8, launch, stream, "enc_intersect_any");
 }
 
 enc_status enc_accel_check(enc_accel a, enc_stream stream) {

@@ -199,6 +199,11 @@ BinSpec make_bin_spec(const float lo[3], const float hi[3], int key_bits, int di
 int launch_bin(const float* d_rays, size_t n, const BinSpec& spec, void* d_scratch,
                uint32_t** d_order, int device, void* stream);
 
+// Writes n rays of 6 floats (origin, direction; 8-byte aligned) as n rays of
+// the 8-float layout with tmin = 0 and tmax = +inf (ray_widen.cu).
+// Asynchronous on `stream`.
+int launch_widen_rays(const float* d_od, size_t n, float* d_rays, int device, void* stream);
+
 // Kernel launchers (trace.cu).  All asynchronous on `stream`.  d_order (may
 // be null): queue index q traces ray d_order[q].
 int launch_closest(const DevAccel& a, const float* d_rays, size_t n, enc_hit* d_hits,

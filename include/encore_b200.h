@@ -210,6 +210,17 @@ enc_status enc_accel_deserialize(const void* buf, size_t size, int32_t device, e
  * `stream` before returning. */
 enc_status enc_intersect_closest(enc_accel accel, const float* rays, size_t nrays, enc_hit* hits,
                                  const enc_launch_opts* launch, enc_stream stream);
+/* AccelerationStructure::intersect (AccelerationStructure.h:63), batched, on
+ * the reference's own ray payload: 6 floats per ray (ox, oy, oz, dx, dy, dz),
+ * a Ray's m_Origin and m_Direction (Ray.h:44-45), which carries no distance
+ * bounds (a hit needs t > 0 only, TrianglePrim.cpp:222-223).  Host buffers,
+ * as enc_intersect_closest; the hits equal that call's on the same rays with
+ * tmin = 0 and tmax = +inf, bit for bit.  24 bytes per ray cross PCIe instead
+ * of 32; each chunk is widened to the 8-float layout in device memory ahead
+ * of its trace. */
+enc_status enc_intersect_closest_od(enc_accel accel, const float* rays, size_t nrays,
+                                    enc_hit* hits, const enc_launch_opts* launch,
+                                    enc_stream stream);
 /* Device-buffer form: rays and hits already in device memory; asynchronous
  * on `stream`.  Kernel status is read by enc_accel_check.  Each launch on an
  * accelerator takes the next of its 256 work-queue heads, so at most 256

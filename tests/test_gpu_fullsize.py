@@ -165,3 +165,25 @@ def test_fullsize_any_hit_is_closest_before_tmax(gpu, workload):
     short = rays[h].copy()
     short[:, 7] = np.nextafter(hits["t"][h], np.float32(0))
     assert not acc.occluded(short).any()
+
+
+def test_origin_direction_form_equals_the_8_float_form(gpu, workload):
+    """enc_intersect_closest_od takes the reference's Ray payload (origin,
+    direction: 24 bytes per ray) and widens it on the device; its hits equal
+    enc_intersect_closest's on the same rays with tmin = 0 and tmax = +inf,
+    bit for bit: the full batch (eight 512K-ray chunks and the short final
+    chunk of the pipeline), an unaligned middle slice, and a one-chunk call."""
+    tris, rays, acc = workload
+    r8 = np.ascontiguousarray(rays, dtype=np.float32).copy()
+    r8[:, 3] = 0.0
+    r8[:, 7] = np.inf
+    od = np.ascontiguousarray(np.concatenate([r8[:, 0:3], r8[:, 4:7]], axis=1))
+    for lo, hi in ((0, len(r8)), (12345, 12345 + 1_500_001), (7, 7 + 777)):
+        want = acc.intersect(r8[lo:hi])
+        got = acc.intersect_od(od[lo:hi])
+        assert np.array_equal(got["tri"], want["tri"]), (lo, hi)
+        for f in ("t", "u", "v"):
+            assert np.array_equal(bits(got[f]), bits(want[f])), (lo, hi, f)
+        # twice in a row: the staging buffers keep the last call's contents
+        again = acc.intersect_od(od[lo:hi])
+        assert np.array_equal(again.view(np.uint8), got.view(np.uint8))
