@@ -25,10 +25,11 @@ struct enc_accel_s {
   void* d_stage_out = nullptr;
   void* d_stage_od = nullptr;  // rays of 6 floats, before widening (enc_intersect_closest_od)
   size_t stage_in_bytes = 0, stage_out_bytes = 0, stage_od_bytes = 0;
-  // host-form pipeline: copy-in, trace and copy-out streams, and per-chunk
-  // events (copy-in done, trace done)
-  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
-  std::vector<cudaEvent_t> ev_in, ev_trace;
+  // host-form pipeline: copy-in, trace, copy-out, ray-widening and second
+  // trace streams, and per-chunk events (copy-in done, trace done, widening
+  // done)
+  cudaStream_t pipe[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> ev_in, ev_trace, ev_wide;
   cudaEvent_t pipe_start = nullptr, pipe_done = nullptr;
 };
 
@@ -623,10 +624,11 @@ enc_status enc_accel_destroy(enc_accel a) {
   cudaFree(a->d_stage_in);
   cudaFree(a->d_stage_od);
   cudaFree(a->d_stage_out);
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 5; ++i)
     if (a->pipe[i]) cudaStreamDestroy(a->pipe[i]);
   for (cudaEvent_t e : a->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : a->ev_trace) cudaEventDestroy(e);
+  for (cudaEvent_t e : a->ev_wide) cudaEventDestroy(e);
   if (a->pipe_start) cudaEventDestroy(a->pipe_start);
   if (a->pipe_done) cudaEventDestroy(a->pipe_done);
   delete a;
@@ -841,8 +843,9 @@ namespace {
 // behind chunk i's copy out, was 15 % slower.)  Ordering with the caller's
 // stream is kept with events; the call returns after the results are in
 // `out`.  ray_floats = 8: rays in the traversal's layout; 6 (closest hit
-// only): origin and direction, copied in at 24 bytes per ray and widened on
-// the trace stream ahead of each chunk's trace.
+// only): origin and direction, copied in at 24 bytes per ray and widened on a
+// fourth stream ahead of each chunk's trace, with the traces alternating
+// between two streams.
 enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, size_t out_bytes,
                      bool any, int ray_floats, const enc_launch_opts* launch, enc_stream stream,
                      const char* what) {
@@ -893,7 +896,7 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     return read_status(a, s);
   }
   if (!a->pipe[0]) {
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 5; ++i)
       ENC_CUDA(cudaStreamCreateWithFlags(&a->pipe[i], cudaStreamNonBlocking), "stream create");
     ENC_CUDA(cudaEventCreateWithFlags(&a->pipe_start, cudaEventDisableTiming), "event create");
     ENC_CUDA(cudaEventCreateWithFlags(&a->pipe_done, cudaEventDisableTiming), "event create");
@@ -909,29 +912,47 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
   bound.push_back(nrays);
   const size_t nch = bound.size() - 1;
   while (a->ev_in.size() < nch) {
-    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    cudaEvent_t e1 = nullptr, e2 = nullptr, e3 = nullptr;
     ENC_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming), "event create");
-    const cudaError_t e = cudaEventCreateWithFlags(&e2, cudaEventDisableTiming);
+    cudaError_t e = cudaEventCreateWithFlags(&e2, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e3, cudaEventDisableTiming);
     if (e != cudaSuccess) {
       cudaEventDestroy(e1);
+      if (e2) cudaEventDestroy(e2);
       return cuda_fail(e, "event create");
     }
     a->ev_in.push_back(e1);
     a->ev_trace.push_back(e2);
+    a->ev_wide.push_back(e3);
   }
-  cudaStream_t cin = a->pipe[0], ctr = a->pipe[1], cout = a->pipe[2];
+  cudaStream_t cin = a->pipe[0], ctr = a->pipe[1], cout = a->pipe[2], cwd = a->pipe[3];
   ENC_CUDA(cudaEventRecord(a->pipe_start, s), "event record");
-  for (int i = 0; i < 3; ++i) ENC_CUDA(cudaStreamWaitEvent(a->pipe[i], a->pipe_start, 0), "wait");
+  for (int i = 0; i < 5; ++i) ENC_CUDA(cudaStreamWaitEvent(a->pipe[i], a->pipe_start, 0), "wait");
   for (size_t c = 0; c < nch; ++c) {
     const size_t b = bound[c], n = bound[c + 1] - b;
     ENC_CUDA(cudaMemcpyAsync(dcopy + b * rb, rays + (size_t)ray_floats * b, n * rb,
                              cudaMemcpyHostToDevice, cin),
              "H2D rays");
     ENC_CUDA(cudaEventRecord(a->ev_in[c], cin), "event record");
+    if (od) {
+      // widened on a stream of its own, so the trace stream runs its traces
+      // back to back (+2 % on the bench batch against widening on the trace
+      // stream)
+      ENC_CUDA(cudaStreamWaitEvent(cwd, a->ev_in[c], 0), "wait");
+      const int e = launch_widen_rays((const float*)(dcopy + b * rb), n, (float*)(din + b * 32),
+                                      a->dev.device, cwd);
+      if (e) return cuda_fail((cudaError_t)e, "ray widen launch");
+      ENC_CUDA(cudaEventRecord(a->ev_wide[c], cwd), "event record");
+    }
   }
   for (size_t c = 0; c < nch; ++c) {
     const size_t b = bound[c], n = bound[c + 1] - b;
-    ENC_CUDA(cudaStreamWaitEvent(ctr, a->ev_in[c], 0), "wait");
+    // 24-byte rays: consecutive chunks alternate between two trace streams,
+    // so a chunk's persistent launch starts while the previous one drains
+    // its last rays (1,693 against 1,517 Mrays/s on the bench batch, four
+    // interleaved rounds on one box).
+    cudaStream_t ctr_c = (od && (c & 1)) ? a->pipe[4] : ctr;
+    ENC_CUDA(cudaStreamWaitEvent(ctr_c, od ? a->ev_wide[c] : a->ev_in[c], 0), "wait");
     // The chunks' traces run beside the copies.  With 32-byte rays the copy
     // in is the bottleneck: the per-lane closest-hit kernel (10 blocks per
     // SM) slows the copies less than the faster warp-cooperative one (the
@@ -942,16 +963,11 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     // chunk runs the cooperative kernel (1,693 against 1,428 Mrays/s on the
     // bench batch, four rounds each).
     L.per_lane = !od && c + 1 < nch;
-    if (od) {
-      const int e = launch_widen_rays((const float*)(dcopy + b * rb), n, (float*)(din + b * 32),
-                                      a->dev.device, ctr);
-      if (e) return cuda_fail((cudaError_t)e, "ray widen launch");
-    }
-    int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr)
+    int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr_c)
                 : launch_closest(a->dev, (const float*)(din + b * 32), n,
-                                 (enc_hit*)(dout + b * sizeof(enc_hit)), L, ctr, nullptr);
+                                 (enc_hit*)(dout + b * sizeof(enc_hit)), L, ctr_c, nullptr);
     if (e) return cuda_fail((cudaError_t)e, "trace launch");
-    ENC_CUDA(cudaEventRecord(a->ev_trace[c], ctr), "event record");
+    ENC_CUDA(cudaEventRecord(a->ev_trace[c], ctr_c), "event record");
     ENC_CUDA(cudaStreamWaitEvent(cout, a->ev_trace[c], 0), "wait");
     ENC_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + b * out_bytes, dout + b * out_bytes,
                              n * out_bytes, cudaMemcpyDeviceToHost, cout),

@@ -44,6 +44,12 @@ def test_errors_without_device_are_reported_not_raised():
     assert b"no triangles" in lib.enc_last_error()
     lib.enc_scene_destroy(s)
     assert lib.enc_accel_build(None, None, 0, C.byref(a)) == _lib.ENC_ERR_INVALID_ARG
+    # the host-buffer queries check their arguments before any device call
+    rays = (C.c_float * 6)()
+    hits = (C.c_int32 * 4)()
+    for fn in (lib.enc_intersect_closest, lib.enc_intersect_closest_od):
+        assert fn(None, rays, 1, hits, None, None) == _lib.ENC_ERR_INVALID_ARG
+        assert b"null argument" in lib.enc_last_error()
 
 
 def test_deserialize_rejects_malformed_images_before_any_device_call():
