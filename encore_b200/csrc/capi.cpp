@@ -949,7 +949,7 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     const size_t b = bound[c], n = bound[c + 1] - b;
     // 24-byte rays: consecutive chunks alternate between two trace streams,
     // so a chunk's persistent launch starts while the previous one drains
-    // its last rays (1,693 against 1,517 Mrays/s on the bench batch, four
+    // its last rays (1,798 against 1,724 Mrays/s on the bench batch, five
     // interleaved rounds on one box).
     cudaStream_t ctr_c = (od && (c & 1)) ? a->pipe[4] : ctr;
     ENC_CUDA(cudaStreamWaitEvent(ctr_c, od ? a->ev_wide[c] : a->ev_in[c], 0), "wait");
