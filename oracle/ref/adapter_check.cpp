@@ -142,6 +142,15 @@ Tally compare(AccelerationStructure& ref, GpuAccel& gpu, const std::vector<float
     const IPrimitive* pb = okb ? hb.hitObject : NULL;
     if (gpu.primitive(hits[i].tri) != pb) ++t.batch_diff;
   }
+  // the batched call on the Ray payload itself (origin, direction) gives the
+  // 8-float batch's hits, field for field
+  std::vector<enc_hit> hits6(n);
+  if (gpu.intersectBatchOD(&rays[0], n, &hits6[0]) != ENC_OK) {
+    t.batch_diff += (long)n;
+    return t;
+  }
+  for (size_t i = 0; i < n; ++i)
+    if (std::memcmp(&hits6[i], &hits[i], sizeof(enc_hit)) != 0) ++t.batch_diff;
   return t;
 }
 

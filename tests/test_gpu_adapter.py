@@ -10,6 +10,9 @@ PhotonMap and on the adapters with the same models, rays and photons:
 * kd mode: every HitInfo field identical (object, t, point, normal,
   isEntering) on every ray, before and after the scene moves;
 * wide-BVH mode: the same primitive, or a tie at the same FP32 t;
+* both modes: the batched 8-float call names the per-ray call's primitive,
+  and the batched call on the Ray payload (origin, direction) returns the
+  8-float batch's hits, field for field;
 * photon maps: the same k-nearest photon sets, a valid max-heap as the
   reference returns, radiance within 1e-4 relative.
 """
