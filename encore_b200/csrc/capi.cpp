@@ -906,7 +906,7 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
   for (size_t c = 0; c < nchunks; ++c) bound.push_back(c * kChunk);
   // A short final chunk: the call ends with the last chunk's trace and copy
   // out, so 64K rays there instead of up to 512K shorten it (+2.5 % on the
-  // 4.18M-ray bench batch, four back-to-back rounds).
+  // 4.18M-ray bench batch, four back-to-back passes).
   const size_t kTail = (size_t)1 << 16;
   if (nrays - bound.back() > kTail) bound.push_back(nrays - kTail);
   bound.push_back(nrays);
@@ -950,7 +950,7 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     // 24-byte rays: consecutive chunks alternate between two trace streams,
     // so a chunk's persistent launch starts while the previous one drains
     // its last rays (1,798 against 1,724 Mrays/s on the bench batch, five
-    // interleaved rounds on one box).
+    // interleaved passes on one box).
     cudaStream_t ctr_c = (od && (c & 1)) ? a->pipe[4] : ctr;
     ENC_CUDA(cudaStreamWaitEvent(ctr_c, od ? a->ev_wide[c] : a->ev_in[c], 0), "wait");
     // The chunks' traces run beside the copies.  With 32-byte rays the copy
@@ -961,7 +961,7 @@ enc_status host_form(enc_accel a, const float* rays, size_t nrays, void* out, si
     // cooperative kernel to shorten the call's tail (+1.4 %).  With 24-byte
     // rays a chunk's copy in is shorter than its per-lane trace, so every
     // chunk runs the cooperative kernel (1,693 against 1,428 Mrays/s on the
-    // bench batch, four rounds each).
+    // bench batch, four passes each).
     L.per_lane = !od && c + 1 < nch;
     int e = any ? launch_any(a->dev, (const float*)(din + b * 32), n, (uint8_t*)(dout + b), L, ctr_c)
                 : launch_closest(a->dev, (const float*)(din + b * 32), n,
