@@ -83,3 +83,18 @@ def test_photonmap_deserialize_rejects_malformed_images():
     assert b"not a serialised photon map" in lib.enc_last_error()
     assert lib.enc_photonmap_deserialize(junk.ctypes.data, 8, 0, C.byref(out)) == _lib.ENC_ERR_INVALID_ARG
     assert not out.value
+
+
+def test_ray_payload_shapes_are_checked_before_any_call():
+    """intersect takes (N, 8) rays and intersect_od (N, 6): the wrong width is
+    a ValueError raised on the host, before the library is called."""
+    import numpy as np
+    import pytest
+    from encore_b200 import Accelerator
+    acc = Accelerator.__new__(Accelerator)
+    acc.lib = _lib.load()
+    acc.handle = None
+    with pytest.raises(ValueError, match="6"):
+        acc.intersect_od(np.zeros((4, 8), np.float32))
+    with pytest.raises(ValueError, match="8"):
+        acc.intersect(np.zeros((4, 6), np.float32))
